@@ -1,0 +1,179 @@
+"""ctypes binding of libpartia_b200.so (the C ABI declared in include/partia_b200.h).
+
+The library is built in-tree by ``_build.py``.  Loading fails loudly when it is missing
+or when no CUDA device is usable: there is no CPU fallback for the hot path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libpartia_b200.so")
+
+PB_OK = 0
+PB_ERR_INVALID = -1
+PB_ERR_CAPACITY = -2
+PB_ERR_CUDA = -3
+PB_ERR_STATE = -4
+PB_ERR_INTERNAL = -6
+PB_FP64 = 0
+PB_FP32C = 1
+PB_PERMUTE_CALLER = 1
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lp = ctypes.POINTER(ctypes.c_int64)
+_up = ctypes.POINTER(ctypes.c_uint64)
+_vp = ctypes.c_void_p
+
+
+class ArgumentError(ValueError):
+    """Julia's ArgumentError (invalid argument values)."""
+
+
+class DimensionMismatch(ValueError):
+    """Julia's DimensionMismatch (length mismatch between columns)."""
+
+
+class CapacityError(ArgumentError):
+    """n exceeds the Int32 node-id capacity (n <= 2^30)."""
+
+
+class DeviceError(RuntimeError):
+    """CUDA runtime failure or a failed device-side consistency check."""
+
+
+class PBInput(ctypes.Structure):
+    _fields_ = [("npart", ctypes.c_int64),
+                ("x", _vp), ("y", _vp), ("z", _vp), ("m", _vp), ("h", _vp), ("rho", _vp),
+                ("ncolumn", ctypes.c_int32), ("quant", ctypes.POINTER(_vp)), ("kernel", ctypes.c_int32)]
+
+
+class PBCatalog(ctypes.Structure):
+    _fields_ = [("n_scalar", ctypes.c_int32), ("scalar_cols", _ip), ("scalar_shepard", _ip),
+                ("n_grad", ctypes.c_int32), ("grad_cols", _ip),
+                ("n_div", ctypes.c_int32), ("div_cols", _ip),
+                ("n_curl", ctypes.c_int32), ("curl_cols", _ip)]
+
+
+EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set_option", "pb_linear_bvh",
+            "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors",
+            "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
+            "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings"]
+
+_lib = None
+
+
+def load():
+    """Load the shared library and declare every entry point's signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libpartia_b200.so is not built (run distorteddustydiscanalysistoolkits_b200/_build.py); "
+                          "the CUDA path has no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    sig = {
+        "pb_create": (ctypes.c_int32, [P(_vp), ctypes.c_int32]),
+        "pb_destroy": (None, [_vp]),
+        "pb_last_error": (ctypes.c_int32, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+        "pb_set_stream": (ctypes.c_int32, [_vp, _vp]),
+        "pb_set_option": (ctypes.c_int32, [_vp, ctypes.c_char_p, ctypes.c_int64]),
+        "pb_linear_bvh": (ctypes.c_int32, [_vp, P(PBInput), ctypes.c_int32]),
+        "pb_export_encoding": (ctypes.c_int32, [_vp, _vp, _vp]),
+        "pb_export_tree": (ctypes.c_int32, [_vp] + [_vp] * 7 + [_ip]),
+        "pb_find_nearest_h": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+        "pb_query_count": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+        "pb_query_neighbors": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+        "pb_interpolate_points": (ctypes.c_int32, [_vp, P(PBCatalog), ctypes.c_int64, _vp, _vp, _vp,
+                                                   ctypes.c_int32, ctypes.c_int32, P(_vp)]),
+        "pb_interpolate_lines": (ctypes.c_int32, [_vp, P(PBCatalog), ctypes.c_int64] + [_vp] * 6 +
+                                 [ctypes.c_int32, ctypes.c_int32, P(_vp)]),
+        "pb_point_samples_interpolation": (ctypes.c_int32, [_vp, P(PBInput), P(PBCatalog), ctypes.c_int64,
+                                                            _vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32,
+                                                            P(_vp), ctypes.c_int32]),
+        "pb_line_samples_interpolation": (ctypes.c_int32, [_vp, P(PBInput), P(PBCatalog), ctypes.c_int64] +
+                                          [_vp] * 6 + [ctypes.c_int32, ctypes.c_int32, P(_vp), ctypes.c_int32]),
+        "pb_launch_count": (ctypes.c_int64, [_vp]),
+        "pb_last_timings": (ctypes.c_int32, [_vp, _dp, _dp, _lp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def ptr(a):
+    """Address of a contiguous float64/int array (numpy, or a torch tensor on any device)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr") and hasattr(a, "is_contiguous"):
+        if not a.is_contiguous():
+            raise ArgumentError("tensor must be contiguous")
+        return a.data_ptr()
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ArgumentError("array must be C-contiguous")
+        return a.ctypes.data
+    raise ArgumentError("unsupported array type %r" % type(a))
+
+
+class Handle:
+    """Owns one pb_handle (device buffers of one particle set stay resident between calls)."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = _vp()
+        rc = self.lib.pb_create(ctypes.byref(h), int(device))
+        if rc != PB_OK:
+            raise DeviceError("pb_create(device=%d) failed (%d): no usable CUDA device" % (device, rc))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def error(self):
+        buf = ctypes.create_string_buffer(4096)
+        self.lib.pb_last_error(self.h, buf, 4096)
+        return buf.value.decode(errors="replace")
+
+    def check(self, rc, what):
+        if rc == PB_OK:
+            return
+        msg = "%s: %s" % (what, self.error())
+        if rc == PB_ERR_CAPACITY:
+            raise CapacityError(msg)
+        if rc == PB_ERR_INVALID:
+            if "KeyError" in msg:
+                raise KeyError(msg)
+            raise ArgumentError(msg)
+        if rc == PB_ERR_STATE:
+            raise ArgumentError(msg)
+        raise DeviceError(msg)
+
+    def set_option(self, name, value):
+        self.check(self.lib.pb_set_option(self.h, name.encode(), int(value)), "pb_set_option")
+
+    def set_stream(self, stream_ptr):
+        self.check(self.lib.pb_set_stream(self.h, stream_ptr), "pb_set_stream")
+
+    def launch_count(self):
+        return self.lib.pb_launch_count(self.h)
+
+    def timings(self):
+        b, i, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+        self.lib.pb_last_timings(self.h, ctypes.byref(b), ctypes.byref(i), ctypes.byref(n))
+        return b.value, i.value, n.value

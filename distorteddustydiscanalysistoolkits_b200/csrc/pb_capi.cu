@@ -1,0 +1,746 @@
+// pb_capi.cu -- the extern "C" boundary of libpartia_b200.so (declared in include/partia_b200.h).
+//
+// Host orchestration only: argument validation with the reference's error classes,
+// host/device pointer detection and staging, catalog planning (a catalog larger than one
+// launch's register budget is split into several traversal launches), device status
+// checks, and optional CUDA-event timing of the build and traversal stages.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "partia_b200.h"
+#include "pb_internal.h"
+
+using namespace pb;
+
+struct pb_handle {
+    Handle H;
+};
+
+pb::Handle::~Handle()
+{
+    DBuf *all[] = {&in_x, &in_y, &in_z, &in_h, &in_m, &in_rho, &codes, &codes_alt, &idx, &idx_alt, &scan_tmp,
+                   &scan_part, &hist, &bbox_part, &qparams, &status, &leaf, &leaf_escape, &node, &node_hmax, &left,
+                   &right, &escape, &parent, &bmin64, &bmax64, &hmax64, &counters, &m_s, &rho_s, &col_ptrs,
+                   &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux};
+    for (DBuf *b : all) b->release();
+    for (auto &b : in_cols) b.release();
+    for (auto &b : cols_s) b.release();
+    for (auto &b : q_outs) b.release();
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+namespace {
+
+int fail(Handle &H, int code, const std::string &msg)
+{
+    H.err = msg;
+    return code;
+}
+
+#define CK(expr)                                                                                     \
+    do {                                                                                             \
+        cudaError_t _e = (expr);                                                                     \
+        if (_e != cudaSuccess)                                                                       \
+            return fail(H, PB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));         \
+    } while (0)
+
+bool is_device_ptr(const void *p)
+{
+    if (!p) return false;
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// device view of a caller array: the array itself if it lives on the device, else a staged copy
+cudaError_t stage_in(Handle &H, DBuf &buf, const void *p, size_t bytes, const void **out)
+{
+    if (is_device_ptr(p)) {
+        *out = p;
+        return cudaSuccess;
+    }
+    cudaError_t e = buf.reserve(bytes);
+    if (e) return e;
+    e = cudaMemcpyAsync(buf.p, p, bytes, cudaMemcpyHostToDevice, H.stream);
+    *out = buf.p;
+    return e;
+}
+
+int check_status(Handle &H)
+{
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream));
+    CK(cudaStreamSynchronize(H.stream));
+    if (st & ST_NONFINITE) return fail(H, PB_ERR_INVALID, "non-finite particle coordinate or smoothing length");
+    if (st & ST_REFIT) return fail(H, PB_ERR_INTERNAL, "LBVH refit: an internal node was not combined exactly twice");
+    if (st & ST_TRAVERSAL) return fail(H, PB_ERR_INTERNAL, "traversal exceeded its iteration bound");
+    if (st & ST_POOL) return fail(H, PB_ERR_INVALID, "neighbour pool offsets too small for a query");
+    return PB_OK;
+}
+
+DevTree make_tree(Handle &H)
+{
+    DevTree T;
+    T.n = H.n;
+    T.root = H.n >= 2 ? 1 : 0;
+    T.leaf = H.leaf.as<double4>();
+    T.leaf_escape = H.leaf_escape.as<int>();
+    T.node = H.node.as<NodeF>();
+    T.node_hmax = H.node_hmax.as<float>();
+    T.m = H.m_s.as<double>();
+    T.rho = H.rho_s.as<double>();
+    T.kernel = H.kernel;
+    T.status = H.status.as<int>();
+    return T;
+}
+
+void ev_record(Handle &H, int i)
+{
+    if (!H.timing) return;
+    if (!H.ev[i]) cudaEventCreate(&H.ev[i]);
+    cudaEventRecord(H.ev[i], H.stream);
+}
+
+float ev_ms(Handle &H, int a, int b)
+{
+    if (!H.timing || !H.ev[a] || !H.ev[b]) return 0.f;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, H.ev[a], H.ev[b]);
+    return ms;
+}
+
+// ---------------------------------------------------------------------------------------
+// catalog planning
+struct Item {
+    int kind;          // 0 scalar, 1 grad, 2 div, 3 curl
+    int cols[3];       // column ids (-1 = density for grads, -2 = rho pseudo column in FP32 mode)
+    int ncols;
+    int shep;
+    int out0;          // first global output index
+};
+
+int validate_catalog(Handle &H, const pb_catalog *c, bool lines)
+{
+    if (!c) return fail(H, PB_ERR_INVALID, "catalog is NULL");
+    if (c->n_scalar < 0 || c->n_grad < 0 || c->n_div < 0 || c->n_curl < 0)
+        return fail(H, PB_ERR_INVALID, "negative catalog count");
+    if (lines && (c->n_grad || c->n_div || c->n_curl))
+        return fail(H, PB_ERR_INVALID, "LineSamples interpolation takes scalar quantities only");
+    auto okcol = [&](int col) { return col >= 0 && col < H.ncol; };
+    for (int i = 0; i < c->n_scalar; ++i)
+        if (!okcol(c->scalar_cols[i])) return fail(H, PB_ERR_INVALID, "scalar column out of range (KeyError)");
+    for (int i = 0; i < c->n_grad; ++i)
+        if (c->grad_cols[i] != -1 && !okcol(c->grad_cols[i]))
+            return fail(H, PB_ERR_INVALID, "gradient column out of range (KeyError)");
+    for (int i = 0; i < 3 * c->n_div; ++i)
+        if (!okcol(c->div_cols[i])) return fail(H, PB_ERR_INVALID, "divergence column out of range (KeyError)");
+    for (int i = 0; i < 3 * c->n_curl; ++i)
+        if (!okcol(c->curl_cols[i])) return fail(H, PB_ERR_INVALID, "curl column out of range (KeyError)");
+    return PB_OK;
+}
+
+std::vector<Item> items_of(const pb_catalog *c, bool fp32)
+{
+    std::vector<Item> it;
+    int o = 0;
+    for (int i = 0; i < c->n_scalar; ++i) {
+        Item x{0, {c->scalar_cols[i], 0, 0}, 1, c->scalar_shepard ? (c->scalar_shepard[i] != 0) : 1, o};
+        it.push_back(x);
+        o += 1;
+    }
+    for (int i = 0; i < c->n_grad; ++i) {
+        int col = c->grad_cols[i];
+        Item x{1, {col, 0, 0}, col == -1 ? 0 : 1, 0, o};
+        if (col == -1 && fp32) { x.cols[0] = -2; x.ncols = 1; }
+        it.push_back(x);
+        o += 3;
+    }
+    for (int i = 0; i < c->n_div; ++i) {
+        Item x{2, {c->div_cols[3 * i], c->div_cols[3 * i + 1], c->div_cols[3 * i + 2]}, 3, 0, o};
+        it.push_back(x);
+        o += 1;
+    }
+    for (int i = 0; i < c->n_curl; ++i) {
+        Item x{3, {c->curl_cols[3 * i], c->curl_cols[3 * i + 1], c->curl_cols[3 * i + 2]}, 3, 0, o};
+        it.push_back(x);
+        o += 3;
+    }
+    return it;
+}
+
+struct Launch {
+    std::vector<int> ucols;
+    std::vector<Item> items;
+    int cnt[4] = {0, 0, 0, 0};
+};
+
+std::vector<Launch> plan(const std::vector<Item> &items)
+{
+    const int lim[4] = {MAXS, MAXG, MAXD, MAXC};
+    std::vector<Launch> out;
+    Launch cur;
+    for (const Item &x : items) {
+        std::vector<int> u = cur.ucols;
+        for (int k = 0; k < x.ncols; ++k)
+            if (std::find(u.begin(), u.end(), x.cols[k]) == u.end()) u.push_back(x.cols[k]);
+        bool fits = (int)u.size() <= MAXU && cur.cnt[x.kind] < lim[x.kind];
+        if (!fits) {
+            out.push_back(cur);
+            cur = Launch();
+            u.clear();
+            for (int k = 0; k < x.ncols; ++k)
+                if (std::find(u.begin(), u.end(), x.cols[k]) == u.end()) u.push_back(x.cols[k]);
+        }
+        cur.ucols = u;
+        cur.items.push_back(x);
+        cur.cnt[x.kind]++;
+    }
+    if (!cur.items.empty()) out.push_back(cur);
+    return out;
+}
+
+int uidx(const Launch &L, int col)
+{
+    for (size_t i = 0; i < L.ucols.size(); ++i)
+        if (L.ucols[i] == col) return (int)i;
+    return -1;
+}
+
+DevCatalog dev_catalog(Handle &H, const Launch &L, double *const *outs)
+{
+    DevCatalog C;
+    memset(&C, 0, sizeof(C));
+    C.nU = (int)L.ucols.size();
+    for (int u = 0; u < C.nU; ++u) {
+        int col = L.ucols[u];
+        C.ucol[u] = col == -2 ? H.rho_s.as<double>() : H.cols_s[col].as<double>();
+    }
+    int l = 0;
+    // kernel writes scalars, grads, divs, curls in that order
+    for (int kind = 0; kind < 4; ++kind) {
+        for (const Item &x : L.items) {
+            if (x.kind != kind) continue;
+            if (kind == 0) {
+                C.s_u[C.n_scalar] = uidx(L, x.cols[0]);
+                C.s_shep[C.n_scalar] = x.shep;
+                C.n_scalar++;
+                C.out[l++] = outs[x.out0];
+            } else if (kind == 1) {
+                C.g_u[C.n_grad] = x.cols[0] == -1 ? -1 : uidx(L, x.cols[0]);
+                C.n_grad++;
+                for (int d = 0; d < 3; ++d) C.out[l++] = outs[x.out0 + d];
+            } else if (kind == 2) {
+                for (int d = 0; d < 3; ++d) C.d_u[C.n_div][d] = uidx(L, x.cols[d]);
+                C.n_div++;
+                C.out[l++] = outs[x.out0];
+            } else {
+                for (int d = 0; d < 3; ++d) C.c_u[C.n_curl][d] = uidx(L, x.cols[d]);
+                C.n_curl++;
+                for (int d = 0; d < 3; ++d) C.out[l++] = outs[x.out0 + d];
+            }
+        }
+    }
+    C.L = l;
+    return C;
+}
+
+int64_t catalog_L(const pb_catalog *c) { return c->n_scalar + 3 * c->n_grad + c->n_div + 3 * c->n_curl; }
+
+// stage output pointers: device outputs are written in place, host outputs via staging
+int stage_outputs(Handle &H, int64_t L, int64_t npts, double *const *out, std::vector<double *> &dev,
+                  std::vector<int> &is_host)
+{
+    dev.assign(L, nullptr);
+    is_host.assign(L, 0);
+    if ((int64_t)H.q_outs.size() < L) H.q_outs.resize(L);
+    for (int64_t l = 0; l < L; ++l) {
+        if (!out || !out[l]) return fail(H, PB_ERR_INVALID, "output pointer is NULL");
+        if (is_device_ptr(out[l])) dev[l] = out[l];
+        else {
+            CK(H.q_outs[l].reserve(sizeof(double) * npts));
+            dev[l] = H.q_outs[l].as<double>();
+            is_host[l] = 1;
+        }
+    }
+    return PB_OK;
+}
+
+int finish_outputs(Handle &H, int64_t L, int64_t npts, double *const *out, const std::vector<double *> &dev,
+                   const std::vector<int> &is_host)
+{
+    for (int64_t l = 0; l < L; ++l)
+        if (is_host[l]) CK(cudaMemcpyAsync(out[l], dev[l], sizeof(double) * npts, cudaMemcpyDeviceToHost, H.stream));
+    return check_status(H);
+}
+
+int stage_queries(Handle &H, int64_t nq, const double *qx, const double *qy, const double *qz, const double **dx,
+                  const double **dy, const double **dz)
+{
+    const void *a, *b, *c;
+    CK(stage_in(H, H.q_x, qx, sizeof(double) * nq, &a));
+    CK(stage_in(H, H.q_y, qy, sizeof(double) * nq, &b));
+    CK(stage_in(H, H.q_z, qz, sizeof(double) * nq, &c));
+    *dx = (const double *)a;
+    *dy = (const double *)b;
+    *dz = (const double *)c;
+    return PB_OK;
+}
+
+// Morton order of the queries (a schedule only; each result goes to its own slot)
+int query_order(Handle &H, int64_t nq, const double *dx, const double *dy, const double *dz, const uint32_t **perm)
+{
+    *perm = nullptr;
+    if (!H.sort_queries || nq < 2) return PB_OK;
+    CK(H.q_keys.reserve(sizeof(uint32_t) * nq));
+    CK(H.q_keys_alt.reserve(sizeof(uint32_t) * nq));
+    CK(H.q_perm.reserve(sizeof(uint32_t) * nq));
+    CK(H.q_perm_alt.reserve(sizeof(uint32_t) * nq));
+    CK(launch_query_codes(&H, nq, dx, dy, dz, H.q_keys.as<uint32_t>(), H.q_perm.as<uint32_t>()));
+    CK(sort_pairs_u32(&H, H.q_keys.as<uint32_t>(), H.q_perm.as<uint32_t>(), H.q_keys_alt.as<uint32_t>(),
+                      H.q_perm_alt.as<uint32_t>(), nq, 30));
+    *perm = H.q_perm.as<uint32_t>();
+    return PB_OK;
+}
+
+int do_build(Handle &H, const pb_input *in, int32_t flags)
+{
+    if (!in) return fail(H, PB_ERR_INVALID, "input is NULL");
+    int64_t n = in->npart;
+    if (n < 1) return fail(H, PB_ERR_INVALID, "BinaryRadixTree: enc.codes must be non-empty (got n=0)");
+    if (n > 1073741824LL) return fail(H, PB_ERR_CAPACITY, "n exceeds the Int32 node-id capacity (n <= 2^30)");
+    if (in->kernel < 0 || in->kernel > 5) return fail(H, PB_ERR_INVALID, "unknown kernel id");
+    if (in->ncolumn < 0 || (in->ncolumn > 0 && !in->quant)) return fail(H, PB_ERR_INVALID, "bad quantity columns");
+    if (!in->x || !in->y || !in->z || !in->m || !in->h || !in->rho)
+        return fail(H, PB_ERR_INVALID, "particle column pointer is NULL");
+    for (int c = 0; c < in->ncolumn; ++c)
+        if (!in->quant[c]) return fail(H, PB_ERR_INVALID, "quantity column pointer is NULL");
+    CK(cudaSetDevice(H.device));
+    H.built = false;
+    const size_t nb = sizeof(double) * n;
+    const void *x, *y, *z, *h, *m, *rho;
+    CK(stage_in(H, H.in_x, in->x, nb, &x));
+    CK(stage_in(H, H.in_y, in->y, nb, &y));
+    CK(stage_in(H, H.in_z, in->z, nb, &z));
+    CK(stage_in(H, H.in_h, in->h, nb, &h));
+    CK(stage_in(H, H.in_m, in->m, nb, &m));
+    CK(stage_in(H, H.in_rho, in->rho, nb, &rho));
+    if ((int)H.in_cols.size() < in->ncolumn) H.in_cols.resize(in->ncolumn);
+    if ((int)H.cols_s.size() < in->ncolumn) H.cols_s.resize(in->ncolumn);
+    std::vector<const double *> cols(in->ncolumn);
+    for (int c = 0; c < in->ncolumn; ++c) {
+        const void *p;
+        CK(stage_in(H, H.in_cols[c], in->quant[c], nb, &p));
+        cols[c] = (const double *)p;
+        CK(H.cols_s[c].reserve(nb));
+    }
+    int64_t nin = n > 1 ? n - 1 : 1, ntot = 2 * n - 1;
+    CK(H.codes.reserve(8 * n));
+    CK(H.codes_alt.reserve(8 * n));
+    CK(H.idx.reserve(4 * n));
+    CK(H.idx_alt.reserve(4 * n));
+    CK(H.leaf.reserve(32 * n));
+    CK(H.leaf_escape.reserve(4 * n));
+    CK(H.node.reserve(sizeof(NodeF) * nin));
+    CK(H.node_hmax.reserve(4 * nin));
+    CK(H.left.reserve(4 * nin));
+    CK(H.right.reserve(4 * nin));
+    CK(H.escape.reserve(4 * ntot));
+    CK(H.parent.reserve(4 * ntot));
+    CK(H.bmin64.reserve(24 * nin));
+    CK(H.bmax64.reserve(24 * nin));
+    CK(H.hmax64.reserve(8 * nin));
+    CK(H.counters.reserve(4 * nin));
+    CK(H.m_s.reserve(nb));
+    CK(H.rho_s.reserve(nb));
+    CK(H.qparams.reserve(sizeof(QuantParams)));
+    CK(H.status.reserve(sizeof(int)));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    ev_record(H, 0);
+    CK(launch_bbox(&H, n, (const double *)x, (const double *)y, (const double *)z, (const double *)h));
+    CK(launch_encode(&H, n, (const double *)x, (const double *)y, (const double *)z));
+    CK(sort_pairs_u64(&H, H.codes.as<uint64_t>(), H.idx.as<uint32_t>(), H.codes_alt.as<uint64_t>(),
+                      H.idx_alt.as<uint32_t>(), n, 63));
+    CK(launch_dedupe(&H, H.codes.as<uint64_t>(), n));
+    CK(launch_gather(&H, n, (const double *)x, (const double *)y, (const double *)z, (const double *)h,
+                     (const double *)m, (const double *)rho, cols));
+    CK(launch_topology(&H, n));
+    ev_record(H, 1);
+    H.n = n;
+    H.ncol = in->ncolumn;
+    H.kernel = in->kernel;
+    int rc = check_status(H);
+    if (rc) return rc;
+    H.t_build_ms = ev_ms(H, 0, 1);
+    if (flags & PB_PERMUTE_CALLER) {
+        // the reference permutes the caller's columns in place (InterpolationInput.jl:211-219)
+        CK(H.q_aux.reserve(nb));
+        const double *srcs[6] = {(const double *)x, (const double *)y, (const double *)z,
+                                 (const double *)m, (const double *)h, (const double *)rho};
+        const double *dsts[6] = {in->x, in->y, in->z, in->m, in->h, in->rho};
+        for (int a = 0; a < 6 + in->ncolumn; ++a) {
+            const double *s = a < 6 ? srcs[a] : cols[a - 6];
+            double *d = const_cast<double *>(a < 6 ? dsts[a] : in->quant[a - 6]);
+            CK(launch_permute_back(&H, n, H.idx.as<uint32_t>(), s, H.q_aux.as<double>()));
+            CK(cudaMemcpyAsync(d, H.q_aux.p, nb, cudaMemcpyDefault, H.stream));
+        }
+        CK(cudaStreamSynchronize(H.stream));
+    }
+    H.built = true;
+    return PB_OK;
+}
+
+int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, const double *qy,
+              const double *qz, int32_t strategy, int32_t precision, double *const *out)
+{
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (strategy < 0 || strategy > 2) return fail(H, PB_ERR_INVALID, "unknown interpolation strategy");
+    if (precision != PB_FP64 && precision != PB_FP32C) return fail(H, PB_ERR_INVALID, "unknown precision mode");
+    int rc = validate_catalog(H, cat, false);
+    if (rc) return rc;
+    if (npts < 0) return fail(H, PB_ERR_INVALID, "negative number of sample points");
+    H.interp_launches = 0;
+    H.t_interp_ms = 0.f;
+    int64_t L = catalog_L(cat);
+    if (npts == 0 || L == 0) return PB_OK;
+    if (!qx || !qy || !qz) return fail(H, PB_ERR_INVALID, "sample coordinate pointer is NULL");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dx, *dy, *dz;
+    if ((rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz))) return rc;
+    std::vector<double *> dev;
+    std::vector<int> is_host;
+    if ((rc = stage_outputs(H, L, npts, out, dev, is_host))) return rc;
+    const uint32_t *perm;
+    if ((rc = query_order(H, npts, dx, dy, dz, &perm))) return rc;
+    DevTree T = make_tree(H);
+    std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
+    ev_record(H, 2);
+    for (const Launch &Lc : launches) {
+        DevCatalog C = dev_catalog(H, Lc, dev.data());
+        if (precision == PB_FP64) CK(launch_points_fp64(&H, T, C, strategy, npts, dx, dy, dz, perm));
+        else CK(launch_points_fp32(&H, T, C, strategy, npts, dx, dy, dz, perm));
+        H.interp_launches++;
+    }
+    ev_record(H, 3);
+    if ((rc = finish_outputs(H, L, npts, out, dev, is_host))) return rc;
+    H.t_interp_ms = ev_ms(H, 2, 3);
+    return PB_OK;
+}
+
+int do_lines(Handle &H, const pb_catalog *cat, int64_t nl, const double *ox, const double *oy, const double *oz,
+             const double *mx, const double *my, const double *mz, int32_t strategy, int32_t precision,
+             double *const *out)
+{
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (strategy != SCATTER)
+        return fail(H, PB_ERR_INVALID,
+                    "LineSamples_interpolation only supports itpScatter (ArgumentError in the reference)");
+    if (precision != PB_FP64 && precision != PB_FP32C) return fail(H, PB_ERR_INVALID, "unknown precision mode");
+    int rc = validate_catalog(H, cat, true);
+    if (rc) return rc;
+    if (nl < 0) return fail(H, PB_ERR_INVALID, "negative number of lines");
+    H.interp_launches = 0;
+    H.t_interp_ms = 0.f;
+    int64_t L = cat->n_scalar;
+    if (nl == 0 || L == 0) return PB_OK;
+    if (!ox || !oy || !oz || !mx || !my || !mz) return fail(H, PB_ERR_INVALID, "line pointer is NULL");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dox, *doy, *doz;
+    if ((rc = stage_queries(H, nl, ox, oy, oz, &dox, &doy, &doz))) return rc;
+    const void *a, *b, *c;
+    CK(H.q_out.reserve(sizeof(double) * 3 * nl));
+    // directions: device views or staged into q_out (3 * nl doubles)
+    double *stage = H.q_out.as<double>();
+    const double *dirs[3] = {mx, my, mz};
+    const void *dv[3];
+    for (int d = 0; d < 3; ++d) {
+        if (is_device_ptr(dirs[d])) dv[d] = dirs[d];
+        else {
+            CK(cudaMemcpyAsync(stage + d * nl, dirs[d], sizeof(double) * nl, cudaMemcpyHostToDevice, H.stream));
+            dv[d] = stage + d * nl;
+        }
+    }
+    a = dv[0]; b = dv[1]; c = dv[2];
+    std::vector<double *> dev;
+    std::vector<int> is_host;
+    if ((rc = stage_outputs(H, L, nl, out, dev, is_host))) return rc;
+    const uint32_t *perm;
+    if ((rc = query_order(H, nl, dox, doy, doz, &perm))) return rc;
+    DevTree T = make_tree(H);
+    std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
+    ev_record(H, 2);
+    for (const Launch &Lc : launches) {
+        DevCatalog C = dev_catalog(H, Lc, dev.data());
+        if (precision == PB_FP64)
+            CK(launch_lines_fp64(&H, T, C, nl, dox, doy, doz, (const double *)a, (const double *)b, (const double *)c, perm));
+        else
+            CK(launch_lines_fp32(&H, T, C, nl, dox, doy, doz, (const double *)a, (const double *)b, (const double *)c, perm));
+        H.interp_launches++;
+    }
+    ev_record(H, 3);
+    if ((rc = finish_outputs(H, L, nl, out, dev, is_host))) return rc;
+    H.t_interp_ms = ev_ms(H, 2, 3);
+    return PB_OK;
+}
+
+}  // namespace
+
+// =========================================================================================
+extern "C" {
+
+int32_t pb_create(pb_handle **out, int32_t device)
+{
+    if (!out) return PB_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PB_ERR_CUDA;
+    }
+    if (device < 0 || device >= ndev) return PB_ERR_INVALID;
+    pb_handle *p = new pb_handle();
+    p->H.device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&p->H.own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete p;
+        return PB_ERR_CUDA;
+    }
+    p->H.stream = p->H.own_stream;
+    *out = p;
+    return PB_OK;
+}
+
+void pb_destroy(pb_handle *h)
+{
+    if (!h) return;
+    cudaSetDevice(h->H.device);
+    if (h->H.stream) cudaStreamSynchronize(h->H.stream);
+    delete h;
+}
+
+int32_t pb_last_error(const pb_handle *h, char *buf, int64_t size)
+{
+    if (!h) return 0;
+    const std::string &e = h->H.err;
+    if (buf && size > 0) {
+        int64_t k = std::min<int64_t>(size - 1, (int64_t)e.size());
+        memcpy(buf, e.data(), k);
+        buf[k] = 0;
+    }
+    return (int32_t)e.size();
+}
+
+int32_t pb_set_stream(pb_handle *h, void *s)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    H.stream = s ? (cudaStream_t)s : H.own_stream;
+    return PB_OK;
+}
+
+int32_t pb_set_option(pb_handle *h, const char *name, int64_t value)
+{
+    if (!h || !name) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!strcmp(name, "timing")) H.timing = value != 0;
+    else if (!strcmp(name, "sort_queries")) H.sort_queries = (int)value;
+    else if (!strcmp(name, "block_size")) H.block_size = (int)value;
+    else return fail(H, PB_ERR_INVALID, std::string("unknown option ") + name);
+    return PB_OK;
+}
+
+int32_t pb_linear_bvh(pb_handle *h, const pb_input *in, int32_t flags)
+{
+    if (!h) return PB_ERR_INVALID;
+    return do_build(h->H, in, flags);
+}
+
+int32_t pb_export_encoding(pb_handle *h, uint64_t *codes, int64_t *order)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    CK(cudaSetDevice(H.device));
+    int64_t n = H.n;
+    if (codes) CK(cudaMemcpyAsync(codes, H.codes.p, 8 * n, cudaMemcpyDefault, H.stream));
+    if (order) {
+        std::vector<uint32_t> tmp(n);
+        CK(cudaMemcpyAsync(tmp.data(), H.idx.p, 4 * n, cudaMemcpyDeviceToHost, H.stream));
+        CK(cudaStreamSynchronize(H.stream));
+        std::vector<int64_t> w(tmp.begin(), tmp.end());
+        CK(cudaMemcpy(order, w.data(), 8 * n, cudaMemcpyDefault));
+    }
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
+
+int32_t pb_export_tree(pb_handle *h, int32_t *left, int32_t *right, int32_t *escape, int32_t *parent, double *bmin,
+                       double *bmax, double *hmax, int32_t *root)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    CK(cudaSetDevice(H.device));
+    int64_t n = H.n, nin = n - 1, ntot = 2 * n - 1;
+    if (root) *root = n >= 2 ? 1 : 0;
+    std::vector<int32_t> z(ntot, 0);
+    if (left) {
+        CK(cudaMemcpy(left, z.data(), 4 * ntot, cudaMemcpyDefault));
+        if (nin > 0) CK(cudaMemcpyAsync(left, H.left.p, 4 * nin, cudaMemcpyDefault, H.stream));
+    }
+    if (right) {
+        CK(cudaMemcpy(right, z.data(), 4 * ntot, cudaMemcpyDefault));
+        if (nin > 0) CK(cudaMemcpyAsync(right, H.right.p, 4 * nin, cudaMemcpyDefault, H.stream));
+    }
+    if (escape) CK(cudaMemcpyAsync(escape, H.escape.p, 4 * ntot, cudaMemcpyDefault, H.stream));
+    if (parent) CK(cudaMemcpyAsync(parent, H.parent.p, 4 * ntot, cudaMemcpyDefault, H.stream));
+    if (nin > 0) {
+        if (bmin) CK(cudaMemcpyAsync(bmin, H.bmin64.p, 24 * nin, cudaMemcpyDefault, H.stream));
+        if (bmax) CK(cudaMemcpyAsync(bmax, H.bmax64.p, 24 * nin, cudaMemcpyDefault, H.stream));
+        if (hmax) CK(cudaMemcpyAsync(hmax, H.hmax64.p, 8 * nin, cudaMemcpyDefault, H.stream));
+    }
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
+
+int32_t pb_find_nearest_h(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                          double *h_out, int64_t *idx_out)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (npts <= 0) return npts == 0 ? PB_OK : fail(H, PB_ERR_INVALID, "negative npts");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dx, *dy, *dz;
+    int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
+    if (rc) return rc;
+    CK(H.q_out.reserve(16 * npts));
+    double *hd = H.q_out.as<double>();
+    int64_t *id = reinterpret_cast<int64_t *>(hd + npts);
+    CK(launch_nearest(&H, make_tree(H), npts, dx, dy, dz, hd, id));
+    if (h_out) CK(cudaMemcpyAsync(h_out, hd, 8 * npts, cudaMemcpyDefault, H.stream));
+    if (idx_out) CK(cudaMemcpyAsync(idx_out, id, 8 * npts, cudaMemcpyDefault, H.stream));
+    return check_status(H);
+}
+
+int32_t pb_query_count(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                       const double *radius, int64_t *counts)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (npts <= 0) return npts == 0 ? PB_OK : fail(H, PB_ERR_INVALID, "negative npts");
+    if (!radius || !counts) return fail(H, PB_ERR_INVALID, "NULL radius/counts");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dx, *dy, *dz;
+    int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
+    if (rc) return rc;
+    const void *r;
+    CK(stage_in(H, H.q_aux, radius, 8 * npts, &r));
+    CK(H.q_out.reserve(8 * npts));
+    CK(launch_query(&H, make_tree(H), npts, dx, dy, dz, (const double *)r, nullptr, H.q_out.as<int64_t>(), nullptr,
+                    nullptr));
+    CK(cudaMemcpyAsync(counts, H.q_out.p, 8 * npts, cudaMemcpyDefault, H.stream));
+    return check_status(H);
+}
+
+int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                           const double *radius, const int64_t *offsets, int64_t *pool, int64_t *nearest)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (npts <= 0) return npts == 0 ? PB_OK : fail(H, PB_ERR_INVALID, "negative npts");
+    if (!radius || !offsets || !pool) return fail(H, PB_ERR_INVALID, "NULL radius/offsets/pool");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dx, *dy, *dz;
+    int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
+    if (rc) return rc;
+    const void *r, *o;
+    CK(stage_in(H, H.q_aux, radius, 8 * npts, &r));
+    CK(stage_in(H, H.q_keys, offsets, 8 * (npts + 1), &o));
+    int64_t total = 0;
+    CK(cudaStreamSynchronize(H.stream));
+    CK(cudaMemcpy(&total, (const int64_t *)o + npts, 8, cudaMemcpyDefault));
+    if (total < 0) return fail(H, PB_ERR_INVALID, "negative pool size");
+    bool pool_dev = is_device_ptr(pool);
+    int64_t *dpool = pool;
+    if (!pool_dev) {
+        CK(H.q_perm_alt.reserve(8 * (total + 1)));
+        dpool = H.q_perm_alt.as<int64_t>();
+    }
+    CK(H.q_out.reserve(8 * npts));
+    CK(launch_query(&H, make_tree(H), npts, dx, dy, dz, (const double *)r, (const int64_t *)o, nullptr, dpool,
+                    H.q_out.as<int64_t>()));
+    if (!pool_dev && total > 0) CK(cudaMemcpyAsync(pool, dpool, 8 * total, cudaMemcpyDeviceToHost, H.stream));
+    if (nearest) CK(cudaMemcpyAsync(nearest, H.q_out.p, 8 * npts, cudaMemcpyDefault, H.stream));
+    return check_status(H);
+}
+
+int32_t pb_interpolate_points(pb_handle *h, const pb_catalog *cat, int64_t npts, const double *qx, const double *qy,
+                              const double *qz, int32_t strategy, int32_t precision, double *const *out)
+{
+    if (!h) return PB_ERR_INVALID;
+    return do_points(h->H, cat, npts, qx, qy, qz, strategy, precision, out);
+}
+
+int32_t pb_interpolate_lines(pb_handle *h, const pb_catalog *cat, int64_t nlines, const double *ox, const double *oy,
+                             const double *oz, const double *dx, const double *dy, const double *dz, int32_t strategy,
+                             int32_t precision, double *const *out)
+{
+    if (!h) return PB_ERR_INVALID;
+    return do_lines(h->H, cat, nlines, ox, oy, oz, dx, dy, dz, strategy, precision, out);
+}
+
+int32_t pb_point_samples_interpolation(pb_handle *h, const pb_input *in, const pb_catalog *cat, int64_t npts,
+                                       const double *qx, const double *qy, const double *qz, int32_t strategy,
+                                       int32_t precision, double *const *out, int32_t flags)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (strategy < 0 || strategy > 2) return fail(H, PB_ERR_INVALID, "unknown interpolation strategy");
+    int rc = do_build(H, in, flags);
+    if (rc) return rc;
+    return do_points(H, cat, npts, qx, qy, qz, strategy, precision, out);
+}
+
+int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb_catalog *cat, int64_t nlines,
+                                      const double *ox, const double *oy, const double *oz, const double *dx,
+                                      const double *dy, const double *dz, int32_t strategy, int32_t precision,
+                                      double *const *out, int32_t flags)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (strategy != SCATTER)
+        return fail(H, PB_ERR_INVALID,
+                    "LineSamples_interpolation only supports itpScatter (ArgumentError in the reference)");
+    int rc = do_build(H, in, flags);
+    if (rc) return rc;
+    return do_lines(H, cat, nlines, ox, oy, oz, dx, dy, dz, strategy, precision, out);
+}
+
+int64_t pb_launch_count(const pb_handle *h) { return h ? h->H.launches : 0; }
+
+int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms, int64_t *interp_launches)
+{
+    if (!h) return PB_ERR_INVALID;
+    if (build_ms) *build_ms = h->H.t_build_ms;
+    if (interp_ms) *interp_ms = h->H.t_interp_ms;
+    if (interp_launches) *interp_launches = h->H.interp_launches;
+    return PB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,123 @@
+// pb_internal.h -- host-side handle and the launchers shared between translation units.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pb_device.cuh"
+
+namespace pb {
+
+// grow-only device buffer
+struct DBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t b)
+    {
+        if (b <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b < 256 ? 256 : b);
+        if (e == cudaSuccess) bytes = b < 256 ? 256 : b;
+        return e;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+struct QuantParams {
+    double vmin[3];
+    double inv[3];
+    int flat[3];   // axis with zero extent: every particle gets f = 0.5
+    int pad;
+};
+
+struct Handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;       // where launches go
+    cudaStream_t own_stream = nullptr;   // created by pb_create
+    std::string err;
+    int64_t launches = 0;
+
+    // built particle set
+    bool built = false;
+    int64_t n = 0;
+    int ncol = 0;
+    int kernel = 0;
+
+    DBuf in_x, in_y, in_z, in_h, in_m, in_rho;    // staging for host inputs
+    std::vector<DBuf> in_cols;
+    DBuf codes, codes_alt, idx, idx_alt, scan_tmp, scan_part, hist;
+    DBuf bbox_part, qparams, status;
+    DBuf leaf, leaf_escape, node, node_hmax;
+    DBuf left, right, escape, parent;
+    DBuf bmin64, bmax64, hmax64, counters;
+    DBuf m_s, rho_s;
+    std::vector<DBuf> cols_s;
+    DBuf col_ptrs;      // device array of sorted column pointers
+
+    // query-side scratch
+    DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
+    std::vector<DBuf> q_outs;
+
+    // timing (CUDA events around the build and the traversal launches)
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    float t_build_ms = 0.f, t_interp_ms = 0.f;
+    int64_t interp_launches = 0;
+    int sort_queries = 1;
+    int block_size = 128;
+
+    ~Handle();
+};
+
+// ---- launchers (pb_build.cu) ----
+cudaError_t launch_bbox(Handle *H, int64_t n, const double *x, const double *y, const double *z, const double *h);
+cudaError_t launch_encode(Handle *H, int64_t n, const double *x, const double *y, const double *z);
+cudaError_t sort_pairs_u64(Handle *H, uint64_t *keys, uint32_t *vals, uint64_t *kalt, uint32_t *valt, int64_t n,
+                           int bits);
+cudaError_t sort_pairs_u32(Handle *H, uint32_t *keys, uint32_t *vals, uint32_t *kalt, uint32_t *valt, int64_t n,
+                           int bits);
+cudaError_t launch_dedupe(Handle *H, uint64_t *codes, int64_t n);
+cudaError_t launch_gather(Handle *H, int64_t n, const double *x, const double *y, const double *z, const double *h,
+                          const double *m, const double *rho, const std::vector<const double *> &cols);
+cudaError_t launch_topology(Handle *H, int64_t n);
+cudaError_t launch_query_codes(Handle *H, int64_t nq, const double *qx, const double *qy, const double *qz,
+                               uint32_t *keys, uint32_t *perm);
+cudaError_t launch_permute_back(Handle *H, int64_t n, const uint32_t *idx, const double *src, double *dst);
+
+// ---- launchers (pb_interp64.cu / pb_interp32.cu / pb_query.cu) ----
+cudaError_t launch_points_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
+                               const double *qx, const double *qy, const double *qz, const uint32_t *perm);
+cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
+                               const double *qx, const double *qy, const double *qz, const uint32_t *perm);
+cudaError_t launch_lines_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int64_t nl, const double *ox,
+                              const double *oy, const double *oz, const double *dx, const double *dy,
+                              const double *dz, const uint32_t *perm);
+cudaError_t launch_lines_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int64_t nl, const double *ox,
+                              const double *oy, const double *oz, const double *dx, const double *dy,
+                              const double *dz, const uint32_t *perm);
+cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
+                           const double *qz, double *h_out, int64_t *idx_out);
+cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
+                         const double *qz, const double *radius, const int64_t *offsets, int64_t *counts,
+                         int64_t *pool, int64_t *nearest);
+cudaError_t upload_line_tables();
+
+inline int grid_for(int64_t n, int block, int cap = 148 * 32)
+{
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+}  // namespace pb

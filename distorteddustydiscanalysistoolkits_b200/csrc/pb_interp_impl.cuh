@@ -1,0 +1,544 @@
+// pb_interp_impl.cuh -- fused nearest-h search + ball-query traversal + SPH kernel sums,
+// one thread per sample point, stackless left/escape DFS (LinearBVHTraversalMacros.jl:26-371).
+//
+// Included by two translation units:
+//   pb_interp64.cu (-fmad=false): Exact64 -- every per-pair term and the finalisation use the
+//       reference's FP64 expressions in the reference's order (general_interpolation.jl,
+//       accumulations/*.jl, kernel.jl), so the results equal the FP64 oracle bit for bit.
+//   pb_interp32.cu: Comp32 -- the same neighbour sets (FP64 distance tests), FP64 pair
+//       offsets, kernel values and per-pair terms in FP32, TwoSum-compensated sums, and an
+//       offset formulation A_b - A_hat for every quantity (A_hat = first accepted neighbour's
+//       value) so that the gradient/divergence/curl differences F - A*B do not cancel in FP32.
+//
+// Accepted neighbours are visited in ascending sorted-leaf order (DFS preorder), exactly as
+// in the reference, so the per-query summation order does not depend on the launch shape.
+// Node pruning uses FP32 boxes rounded outward: it visits a superset of the reference's
+// nodes and accepts exactly the same leaves.
+#pragma once
+#include "pb_device.cuh"
+
+namespace pb {
+
+template <int N, typename T>
+__device__ __forceinline__ T pick(const T (&a)[N], int i)
+{
+    T r = a[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k)
+        if (i == k) r = a[k];
+    return r;
+}
+
+__device__ __forceinline__ void flag(int *status, int bit) { atomicOr(status, bit); }
+
+// LBVH_find_nearest_h (LinearBVHQueries.jl:118-140): min squared distance, first in DFS order
+// (= smallest sorted leaf index) among ties.
+__device__ __forceinline__ int64_t nearest_leaf(const DevTree &T, double px, double py, double pz)
+{
+    double best = INFINITY;
+    int64_t bi = -1;
+    const int64_t n = T.n;
+    if (T.root == 0) {
+        double d2 = d2_point(px, py, pz, ldg4(T.leaf));
+        if (d2 < best) bi = 0;
+        return bi;
+    }
+    int node = T.root;
+    int64_t guard = 0, limit = 4 * n + 64;
+    while (node != 0) {
+        if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
+        if (node >= n) {
+            int64_t b = node - n;
+            double4 L = ldg4(T.leaf + b);
+            int esc = __ldg(T.leaf_escape + b);
+            double d2 = d2_point(px, py, pz, L);
+            if (d2 < best) { best = d2; bi = b; }
+            node = esc;
+        } else {
+            const float4 *np = reinterpret_cast<const float4 *>(T.node + (node - 1));
+            float4 a = __ldg(np), c = __ldg(np + 1);
+            NodeF nd;
+            nd.lox = a.x; nd.loy = a.y; nd.loz = a.z; nd.left = __float_as_int(a.w);
+            nd.hix = c.x; nd.hiy = c.y; nd.hiz = c.z; nd.escape = __float_as_int(c.w);
+            node = (d2_box(px, py, pz, nd) > best) ? nd.escape : nd.left;
+        }
+    }
+    return bi;
+}
+
+__device__ __forceinline__ NodeF load_node(const NodeF *p)
+{
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+    float4 a = __ldg(q), c = __ldg(q + 1);
+    NodeF nd;
+    nd.lox = a.x; nd.loy = a.y; nd.loz = a.z; nd.left = __float_as_int(a.w);
+    nd.hix = c.x; nd.hiy = c.y; nd.hiz = c.z; nd.escape = __float_as_int(c.w);
+    return nd;
+}
+
+// --------------------------------------------------------------------------------------
+// Exact FP64 accumulator (the reference's arithmetic)
+template <int STRAT>
+struct Exact64 {
+    double S1;
+    double SA[MAXU];
+    double Bq[3];
+    double Fg[MAXG][3];
+    double Bd[3], Sd;
+    double D[MAXD];
+    double Cc[MAXC][3];
+
+    __device__ __forceinline__ void init()
+    {
+        S1 = 0.0;
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) SA[u] = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { Bq[d] = 0.0; Bd[d] = 0.0; }
+        Sd = 0.0;
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) Fg[j][0] = Fg[j][1] = Fg[j][2] = 0.0;
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) D[j] = 0.0;
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) Cc[j][0] = Cc[j][1] = Cc[j][2] = 0.0;
+    }
+
+    __device__ __forceinline__ void add(const DevTree &T, const DevCatalog &C, bool need_grad, double px, double py,
+                                        double pz, const double4 &L, int64_t b, double d2, double ha, double hb)
+    {
+        const int k = T.kernel;
+        double dx = px - L.x, dy = py - L.y, dz = pz - L.z;
+        double dr = sqrt(d2);
+        double mb = __ldg(T.m + b), rb = __ldg(T.rho + b);
+        double W;
+        if (STRAT == SYMMETRIC) W = 0.5 * (Wfun<double>(k, dr, ha) + Wfun<double>(k, dr, hb));
+        else W = Wfun<double>(k, dr, STRAT == GATHER ? ha : hb);
+        double w = mb * W / rb;
+        S1 += w;
+        double A[MAXU];
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) {
+            A[u] = (u < C.nU) ? __ldg(C.ucol[u] + b) : 0.0;
+            if (u < C.nU) SA[u] += A[u] * w;
+        }
+        if (!need_grad) return;
+        double gx, gy, gz;
+        if (STRAT == SYMMETRIC) {
+            double ax, ay, az, bx, by, bz;
+            gradW<double>(k, dx, dy, dz, dr, ha, ax, ay, az);
+            gradW<double>(k, dx, dy, dz, dr, hb, bx, by, bz);
+            gx = 0.5 * (ax + bx); gy = 0.5 * (ay + by); gz = 0.5 * (az + bz);
+        } else {
+            gradW<double>(k, dx, dy, dz, dr, STRAT == GATHER ? ha : hb, gx, gy, gz);
+        }
+        double invrb = 1.0 / rb;
+        double ml = mb * invrb;
+        double qx = ml * gx, qy = ml * gy, qz = ml * gz;
+        Bq[0] += qx; Bq[1] += qy; Bq[2] += qz;
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) {
+            if (j < C.n_grad) {
+                int u = C.g_u[j];
+                if (u < 0) {   // density gradient (gradient_accumulation.jl:160-182)
+                    double mx = mb * gx, my = mb * gy, mz = mb * gz;
+                    Fg[j][0] += mx; Fg[j][1] += my; Fg[j][2] += mz;
+                    Bd[0] += mx * invrb; Bd[1] += my * invrb; Bd[2] += mz * invrb;
+                    Sd += mb * W;
+                } else {
+                    double a = pick<MAXU>(A, u);
+                    Fg[j][0] += qx * a; Fg[j][1] += qy * a; Fg[j][2] += qz * a;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) {
+            if (j < C.n_div) {
+                double ax = pick<MAXU>(A, C.d_u[j][0]), ay = pick<MAXU>(A, C.d_u[j][1]), az = pick<MAXU>(A, C.d_u[j][2]);
+                D[j] += qx * ax + qy * ay + qz * az;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) {
+            if (j < C.n_curl) {
+                double ax = pick<MAXU>(A, C.c_u[j][0]), ay = pick<MAXU>(A, C.c_u[j][1]), az = pick<MAXU>(A, C.c_u[j][2]);
+                Cc[j][0] += ay * qz - az * qy;
+                Cc[j][1] += az * qx - ax * qz;
+                Cc[j][2] += ax * qy - ay * qx;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void finalize(const DevCatalog &C, int64_t qi) const
+    {
+        int l = 0;
+        if (S1 == 0.0) {
+            for (int o = 0; o < C.L; ++o) C.out[o][qi] = __longlong_as_double(0x7ff8000000000000LL);
+            return;
+        }
+        double inv = 1.0 / S1;
+#pragma unroll
+        for (int j = 0; j < MAXS; ++j) {
+            if (j < C.n_scalar) {
+                double s = pick<MAXU>(SA, C.s_u[j]);
+                C.out[l++][qi] = C.s_shep[j] ? s * inv : s;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) {
+            if (j < C.n_grad) {
+                int u = C.g_u[j];
+                if (u < 0) {
+                    double a = Sd * inv;
+                    C.out[l++][qi] = Fg[j][0] - Bd[0] * a;
+                    C.out[l++][qi] = Fg[j][1] - Bd[1] * a;
+                    C.out[l++][qi] = Fg[j][2] - Bd[2] * a;
+                } else {
+                    double a = pick<MAXU>(SA, u) * inv;
+                    C.out[l++][qi] = Fg[j][0] - Bq[0] * a;
+                    C.out[l++][qi] = Fg[j][1] - Bq[1] * a;
+                    C.out[l++][qi] = Fg[j][2] - Bq[2] * a;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) {
+            if (j < C.n_div) {
+                double ax = pick<MAXU>(SA, C.d_u[j][0]) * inv;
+                double ay = pick<MAXU>(SA, C.d_u[j][1]) * inv;
+                double az = pick<MAXU>(SA, C.d_u[j][2]) * inv;
+                double bb = ax * Bq[0] + ay * Bq[1] + az * Bq[2];
+                C.out[l++][qi] = D[j] - bb;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) {
+            if (j < C.n_curl) {
+                double ax = pick<MAXU>(SA, C.c_u[j][0]) * inv;
+                double ay = pick<MAXU>(SA, C.c_u[j][1]) * inv;
+                double az = pick<MAXU>(SA, C.c_u[j][2]) * inv;
+                double bx = ay * Bq[2] - az * Bq[1];
+                double by = az * Bq[0] - ax * Bq[2];
+                double bz = ax * Bq[1] - ay * Bq[0];
+                C.out[l++][qi] = -(Cc[j][0] - bx);
+                C.out[l++][qi] = -(Cc[j][1] - by);
+                C.out[l++][qi] = -(Cc[j][2] - bz);
+            }
+        }
+    }
+};
+
+// --------------------------------------------------------------------------------------
+// FP32 compensated accumulator
+template <int STRAT>
+struct Comp32 {
+    CSum S1;
+    CSum SA[MAXU];
+    CSum Bq[3];
+    CSum Fg[MAXG][3];
+    CSum D[MAXD];
+    CSum Cc[MAXC][3];
+    double Ahat[MAXU];
+    bool have;
+
+    __device__ __forceinline__ void init()
+    {
+        S1.zero();
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) { SA[u].zero(); Ahat[u] = 0.0; }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Bq[d].zero();
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) { Fg[j][0].zero(); Fg[j][1].zero(); Fg[j][2].zero(); }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) D[j].zero();
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) { Cc[j][0].zero(); Cc[j][1].zero(); Cc[j][2].zero(); }
+        have = false;
+    }
+
+    __device__ __forceinline__ void add(const DevTree &T, const DevCatalog &C, bool need_grad, double px, double py,
+                                        double pz, const double4 &L, int64_t b, double d2, double ha, double hb)
+    {
+        const int k = T.kernel;
+        float dx = (float)(px - L.x), dy = (float)(py - L.y), dz = (float)(pz - L.z);
+        float dr = sqrtf((float)d2);
+        float mb = (float)__ldg(T.m + b), rb = (float)__ldg(T.rho + b);
+        float fha = (float)ha, fhb = (float)hb;
+        float W;
+        if (STRAT == SYMMETRIC) W = 0.5f * (Wfun<float>(k, dr, fha) + Wfun<float>(k, dr, fhb));
+        else W = Wfun<float>(k, dr, STRAT == GATHER ? fha : fhb);
+        float w = mb * W / rb;
+        S1.add(w);
+        float a[MAXU];
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) {
+            double A = (u < C.nU) ? __ldg(C.ucol[u] + b) : 0.0;
+            if (!have) Ahat[u] = A;
+            a[u] = (float)(A - Ahat[u]);
+            if (u < C.nU) SA[u].add(a[u] * w);
+        }
+        have = true;
+        if (!need_grad) return;
+        float gx, gy, gz;
+        if (STRAT == SYMMETRIC) {
+            float ax, ay, az, bx, by, bz;
+            gradW<float>(k, dx, dy, dz, dr, fha, ax, ay, az);
+            gradW<float>(k, dx, dy, dz, dr, fhb, bx, by, bz);
+            gx = 0.5f * (ax + bx); gy = 0.5f * (ay + by); gz = 0.5f * (az + bz);
+        } else {
+            gradW<float>(k, dx, dy, dz, dr, STRAT == GATHER ? fha : fhb, gx, gy, gz);
+        }
+        float ml = mb / rb;
+        float qx = ml * gx, qy = ml * gy, qz = ml * gz;
+        Bq[0].add(qx); Bq[1].add(qy); Bq[2].add(qz);
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) {
+            if (j < C.n_grad) {
+                float av = pick<MAXU>(a, C.g_u[j]);
+                Fg[j][0].add(qx * av); Fg[j][1].add(qy * av); Fg[j][2].add(qz * av);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) {
+            if (j < C.n_div) {
+                float ax = pick<MAXU>(a, C.d_u[j][0]), ay = pick<MAXU>(a, C.d_u[j][1]), az = pick<MAXU>(a, C.d_u[j][2]);
+                D[j].add(qx * ax + qy * ay + qz * az);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) {
+            if (j < C.n_curl) {
+                float ax = pick<MAXU>(a, C.c_u[j][0]), ay = pick<MAXU>(a, C.c_u[j][1]), az = pick<MAXU>(a, C.c_u[j][2]);
+                Cc[j][0].add(ay * qz - az * qy);
+                Cc[j][1].add(az * qx - ax * qz);
+                Cc[j][2].add(ax * qy - ay * qx);
+            }
+        }
+    }
+
+    __device__ __forceinline__ void finalize(const DevCatalog &C, int64_t qi) const
+    {
+        int l = 0;
+        double S = S1.val();
+        if (S == 0.0) {
+            for (int o = 0; o < C.L; ++o) C.out[o][qi] = __longlong_as_double(0x7ff8000000000000LL);
+            return;
+        }
+        double abar[MAXU];
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) abar[u] = SA[u].val() / S;
+        double B[3] = {Bq[0].val(), Bq[1].val(), Bq[2].val()};
+#pragma unroll
+        for (int j = 0; j < MAXS; ++j) {
+            if (j < C.n_scalar) {
+                int u = C.s_u[j];
+                double ah = pick<MAXU>(Ahat, u);
+                C.out[l++][qi] = C.s_shep[j] ? ah + pick<MAXU>(abar, u) : ah * S + pick<MAXU>(abar, u) * S;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) {
+            if (j < C.n_grad) {
+                double a = pick<MAXU>(abar, C.g_u[j]);
+                C.out[l++][qi] = Fg[j][0].val() - a * B[0];
+                C.out[l++][qi] = Fg[j][1].val() - a * B[1];
+                C.out[l++][qi] = Fg[j][2].val() - a * B[2];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) {
+            if (j < C.n_div) {
+                double ax = pick<MAXU>(abar, C.d_u[j][0]), ay = pick<MAXU>(abar, C.d_u[j][1]),
+                       az = pick<MAXU>(abar, C.d_u[j][2]);
+                C.out[l++][qi] = D[j].val() - (ax * B[0] + ay * B[1] + az * B[2]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) {
+            if (j < C.n_curl) {
+                double ax = pick<MAXU>(abar, C.c_u[j][0]), ay = pick<MAXU>(abar, C.c_u[j][1]),
+                       az = pick<MAXU>(abar, C.c_u[j][2]);
+                double bx = ay * B[2] - az * B[1];
+                double by = az * B[0] - ax * B[2];
+                double bz = ax * B[1] - ay * B[0];
+                C.out[l++][qi] = -(Cc[j][0].val() - bx);
+                C.out[l++][qi] = -(Cc[j][1].val() - by);
+                C.out[l++][qi] = -(Cc[j][2].val() - bz);
+            }
+        }
+    }
+};
+
+// --------------------------------------------------------------------------------------
+// point-sample kernel: one thread per (Morton-ordered) sample point
+template <template <int> class ACC, int STRAT>
+__global__ void __launch_bounds__(128) k_points(DevTree T, DevCatalog C, int64_t nq, const double *__restrict__ qx,
+                                                const double *__restrict__ qy, const double *__restrict__ qz,
+                                                const uint32_t *__restrict__ perm)
+{
+    const int64_t n = T.n;
+    const double K = kernel_valid(T.kernel);
+    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nq; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t qi = perm ? (int64_t)__ldg(perm + j) : j;
+        if (qi >= nq) continue;   // unreachable for a valid permutation
+        double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        double ha = 0.0;
+        if (STRAT != SCATTER) {
+            int64_t b = nearest_leaf(T, px, py, pz);
+            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
+        }
+        double ra = __dmul_rn(K, ha);
+        double r2a = __dmul_rn(ra, ra);
+        ACC<STRAT> acc;
+        acc.init();
+        if (T.root == 0) {
+            double4 L = ldg4(T.leaf);
+            double rr = __dmul_rn(__dmul_rn(K, L.w), __dmul_rn(K, L.w));
+            double r2 = STRAT == GATHER ? r2a : (STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr));
+            double d2 = d2_point(px, py, pz, L);
+            if (d2 <= r2) acc.add(T, C, need_grad, px, py, pz, L, 0, d2, ha, L.w);
+        } else {
+            int node = T.root;
+            int64_t guard = 0, limit = 4 * n + 64;
+            while (node != 0) {
+                if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
+                if (node >= n) {
+                    int64_t b = node - n;
+                    double4 L = ldg4(T.leaf + b);
+                    int esc = __ldg(T.leaf_escape + b);
+                    double r2;
+                    if (STRAT == GATHER) r2 = r2a;
+                    else {
+                        double r = __dmul_rn(K, L.w);
+                        double rr = __dmul_rn(r, r);
+                        r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+                    }
+                    double d2 = d2_point(px, py, pz, L);
+                    if (d2 <= r2) acc.add(T, C, need_grad, px, py, pz, L, b, d2, ha, L.w);
+                    node = esc;
+                } else {
+                    NodeF nd = load_node(T.node + (node - 1));
+                    double r2;
+                    if (STRAT == GATHER) r2 = r2a;
+                    else {
+                        double r = __dmul_rn(K, (double)__ldg(T.node_hmax + (node - 1)));
+                        double rr = __dmul_rn(r, r);
+                        r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+                    }
+                    node = (d2_box(px, py, pz, nd) > r2) ? nd.escape : nd.left;
+                }
+            }
+        }
+        acc.finalize(C, qi);
+    }
+}
+
+// --------------------------------------------------------------------------------------
+// line-sample kernel (itpScatter): one thread per line
+template <typename R>
+__device__ __forceinline__ R line_lut(const R *__restrict__ I, R qmax, R q)
+{
+    const R dq = qmax / R(PB_LINE_NTAB_DEV - 1);
+    R idxf = q / dq + R(1);
+    int i = (int)idxf;
+    i = i < 1 ? 1 : (i > PB_LINE_NTAB_DEV - 1 ? PB_LINE_NTAB_DEV - 1 : i);
+    R t = idxf - R(i);
+    return __ldg(I + i - 1) * (R(1) - t) + __ldg(I + i) * t;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_lines(DevTree T, DevCatalog C, int64_t nl, const double *__restrict__ ox,
+                                               const double *__restrict__ oy, const double *__restrict__ oz,
+                                               const double *__restrict__ mx, const double *__restrict__ my,
+                                               const double *__restrict__ mz, const uint32_t *__restrict__ perm,
+                                               const R *__restrict__ table)
+{
+    const int64_t n = T.n;
+    const int k = T.kernel;
+    const double K = kernel_valid(k);
+    const R qmax = (R)K;
+    const R *I = table + (int64_t)k * PB_LINE_NTAB_DEV;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nl; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t li = perm ? (int64_t)__ldg(perm + j) : j;
+        if (li >= nl) continue;
+        double o[3] = {__ldg(ox + li), __ldg(oy + li), __ldg(oz + li)};
+        double m[3] = {__ldg(mx + li), __ldg(my + li), __ldg(mz + li)};
+        // FP64 mode: plain sums in the reference order; FP32 mode: compensated with offsets
+        double S1 = 0.0, acc[MAXS];
+        CSum cS1, cacc[MAXS];
+        double Ahat[MAXS];
+        bool have = false;
+        cS1.zero();
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) { acc[s] = 0.0; cacc[s].zero(); Ahat[s] = 0.0; }
+        int node = T.root;
+        int64_t bi = 0, guard = 0, limit = 4 * n + 64;
+        bool brute = (node == 0);
+        while (brute ? (bi < n) : (node != 0)) {
+            if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
+            bool leafnode = brute || node >= n;
+            if (leafnode) {
+                int64_t b = brute ? bi++ : (int64_t)(node - n);
+                double4 L = ldg4(T.leaf + b);
+                int esc = brute ? 0 : __ldg(T.leaf_escape + b);
+                double r = __dmul_rn(K, L.w);
+                double r2 = __dmul_rn(r, r);
+                double d2 = d2_line(L.x, L.y, L.z, o, m);
+                if (d2 <= r2) {
+                    double mb = __ldg(T.m + b), rb = __ldg(T.rho + b);
+                    if (sizeof(R) == 8) {
+                        // line_integrated_kernel_function (line_integrated_kernel.jl:132-137)
+                        double dr = sqrt(d2 > 0.0 ? d2 : 0.0);
+                        double invh = 1.0 / L.w;
+                        double q = dr * invh;
+                        double Iq = (q >= K) ? 0.0 : (double)line_lut<R>(I, qmax, (R)q);
+                        double W = invh * Iq;
+                        double w = mb * W / rb;
+                        S1 += w;
+#pragma unroll
+                        for (int s = 0; s < MAXS; ++s)
+                            if (s < C.n_scalar) acc[s] += __ldg(C.ucol[C.s_u[s]] + b) * w;
+                    } else {
+                        float dr = sqrtf(d2 > 0.0 ? (float)d2 : 0.f);
+                        float invh = 1.f / (float)L.w;
+                        float q = dr * invh;
+                        float Iq = (q >= (float)K) ? 0.f : (float)line_lut<R>(I, qmax, (R)q);
+                        float w = (float)mb * (invh * Iq) / (float)rb;
+                        cS1.add(w);
+#pragma unroll
+                        for (int s = 0; s < MAXS; ++s) {
+                            if (s < C.n_scalar) {
+                                double A = __ldg(C.ucol[C.s_u[s]] + b);
+                                if (!have) Ahat[s] = A;
+                                cacc[s].add((float)(A - Ahat[s]) * w);
+                            }
+                        }
+                        have = true;
+                    }
+                }
+                if (!brute) node = esc;
+            } else {
+                NodeF nd = load_node(T.node + (node - 1));
+                double r = __dmul_rn(K, (double)__ldg(T.node_hmax + (node - 1)));
+                double r2 = __dmul_rn(r, r);
+                node = (d2_line_box_lower(o, m, nd) > r2) ? nd.escape : nd.left;
+            }
+        }
+        double S = (sizeof(R) == 8) ? S1 : cS1.val();
+        int l = 0;
+#pragma unroll
+        for (int s = 0; s < MAXS; ++s) {
+            if (s < C.n_scalar) {
+                double v;
+                if (S == 0.0) v = __longlong_as_double(0x7ff8000000000000LL);
+                else if (sizeof(R) == 8) v = C.s_shep[s] ? acc[s] * (1.0 / S) : acc[s];
+                else v = C.s_shep[s] ? Ahat[s] + cacc[s].val() / S : Ahat[s] * S + cacc[s].val();
+                C.out[l++][li] = v;
+            }
+        }
+    }
+}
+
+}  // namespace pb

@@ -1,0 +1,82 @@
+// pb_query.cu -- batched neighbour-search entry points on a built LBVH:
+//   LBVH_find_nearest_h / LBVH_find_nearest (LinearBVHQueries.jl:79-140)
+//   LBVH_query! (LinearBVHQueries.jl:183-211) as count + fill passes (CSR output)
+// These are the bit-exact probes of the neighbour sets: the traversal is the same
+// conservative stackless DFS as the interpolation kernels, so accepted leaves appear in
+// ascending sorted-leaf order exactly as in the reference.
+#include "pb_internal.h"
+#include "pb_interp_impl.cuh"
+
+namespace pb {
+
+__global__ void k_nearest(DevTree T, int64_t nq, const double *__restrict__ qx, const double *__restrict__ qy,
+                          const double *__restrict__ qz, double *h_out, int64_t *idx_out)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t b = nearest_leaf(T, qx[i], qy[i], qz[i]);
+        if (h_out) h_out[i] = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : T.leaf[b].w;
+        if (idx_out) idx_out[i] = b;
+    }
+}
+
+// gather predicate d2 <= radius^2 (LinearBVHTraversalMacros.jl:26-108); pool == nullptr counts only
+__global__ void k_query(DevTree T, int64_t nq, const double *__restrict__ qx, const double *__restrict__ qy,
+                        const double *__restrict__ qz, const double *__restrict__ radius,
+                        const int64_t *__restrict__ offsets, int64_t *counts, int64_t *pool, int64_t *nearest)
+{
+    const int64_t n = T.n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x) {
+        double px = qx[i], py = qy[i], pz = qz[i];
+        double r = radius[i];
+        double r2 = __dmul_rn(r, r);
+        int64_t cnt = 0, ci = -1;
+        double cd = INFINITY;
+        int64_t base = pool ? offsets[i] : 0;
+        int64_t cap = pool ? offsets[i + 1] - offsets[i] : 0;
+        int node = T.root;
+        int64_t bi = 0, guard = 0, limit = 4 * n + 64;
+        bool brute = (node == 0);
+        while (brute ? (bi < n) : (node != 0)) {
+            if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
+            if (brute || node >= n) {
+                int64_t b = brute ? bi++ : (int64_t)(node - n);
+                double4 L = ldg4(T.leaf + b);
+                double d2 = d2_point(px, py, pz, L);
+                if (d2 <= r2) {
+                    if (pool) {
+                        if (cnt < cap) pool[base + cnt] = b;
+                        else flag(T.status, ST_POOL);
+                    }
+                    ++cnt;
+                    if (d2 < cd) { cd = d2; ci = b; }
+                }
+                if (!brute) node = __ldg(T.leaf_escape + b);
+            } else {
+                NodeF nd = load_node(T.node + (node - 1));
+                node = (d2_box(px, py, pz, nd) > r2) ? nd.escape : nd.left;
+            }
+        }
+        if (counts) counts[i] = cnt;
+        if (nearest) nearest[i] = ci;
+    }
+}
+
+cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
+                           const double *qz, double *h_out, int64_t *idx_out)
+{
+    k_nearest<<<grid_for(nq, 128, 1 << 30), 128, 0, H->stream>>>(T, nq, qx, qy, qz, h_out, idx_out);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
+                         const double *qz, const double *radius, const int64_t *offsets, int64_t *counts,
+                         int64_t *pool, int64_t *nearest)
+{
+    k_query<<<grid_for(nq, 128, 1 << 30), 128, 0, H->stream>>>(T, nq, qx, qy, qz, radius, offsets, counts, pool,
+                                                                nearest);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace pb

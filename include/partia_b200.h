@@ -1,0 +1,151 @@
+/*
+ * partia_b200.h -- C ABI of libpartia_b200.so, the B200 (sm_100a) implementation of
+ * Partia.jl's LBVH build + SPH grid interpolation path.
+ *
+ * This is the boundary that Partia's CUDA package extension binds through `ccall`
+ * (Partia.jl/ext/CUDAExt.jl, Partia.jl/src/julia/ExtDummy/CUDAExtDummy.jlh:12).  All
+ * arguments are plain pointers and sizes.  Every pointer may refer to host memory or to
+ * device memory of the handle's device; the library detects which
+ * (cudaPointerGetAttributes) and copies host buffers in and out itself.  Calls are
+ * synchronous, like the reference extension (`CUDA.synchronize()` in
+ * Partia.jl/ext/CUDAExt/KernelInterpolation/grid_interpolation/PointSamples_interpolation.jl:23),
+ * and a handle must be used by one host thread at a time.  No exceptions cross the ABI:
+ * every entry point returns PB_OK or a negative error class, and pb_last_error() holds a
+ * message.  There is no CPU fallback: without a usable CUDA device pb_create fails.
+ *
+ * Conventions (reference -> ABI):
+ *   - indices are 0-based (the Julia shim subtracts 1);
+ *   - tree node ids keep the reference's unified 1-based id space (internal 1..n-1,
+ *     leaf n..2n-1, 0 = none; BinaryRadixTree.jl:36-51); id k is at array index k-1;
+ *   - catalog gradient slot 0 (density gradient, general_interpolation.jl:76-81) is -1;
+ *   - kernels: 0 M4_spline, 1 M5_spline, 2 M6_spline, 3 C2_Wendland, 4 C4_Wendland,
+ *     5 C6_Wendland; strategies: 0 itpGather, 1 itpScatter, 2 itpSymmetric
+ *     (InterpolationStrategy.jl:1-5);
+ *   - precision: PB_FP64 reproduces the reference's Float64 arithmetic in the reference's
+ *     operation order; PB_FP32C runs the kernel sums in FP32 with compensated
+ *     (TwoSum) accumulation and FP64 pair offsets, with the same neighbour sets.
+ */
+#ifndef PARTIA_B200_H
+#define PARTIA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB_OK 0
+#define PB_ERR_INVALID (-1)   /* ArgumentError / DimensionMismatch / bad enum / non-finite coordinate */
+#define PB_ERR_CAPACITY (-2)  /* n > 2^30 (BinaryRadixTree.jl:89-90) */
+#define PB_ERR_CUDA (-3)      /* CUDA runtime error (message in pb_last_error) */
+#define PB_ERR_STATE (-4)     /* query before pb_linear_bvh */
+#define PB_ERR_INTERNAL (-6)  /* device consistency check failed (refit counters, traversal bound) */
+
+#define PB_FP64 0
+#define PB_FP32C 1
+
+/* flags for pb_linear_bvh / pb_*_samples_interpolation */
+#define PB_PERMUTE_CALLER 1   /* permute the caller's particle arrays in place, as LinearBVH! does */
+
+typedef struct pb_handle pb_handle;
+
+/* InterpolationInput{3,Float64} (Partia.jl/src/julia/KernelInterpolation/interpolation_setup/InterpolationInput.jl:43-51) */
+typedef struct {
+    int64_t npart;
+    const double *x, *y, *z, *m, *h, *rho;
+    int32_t ncolumn;
+    const double *const *quant;   /* ncolumn column pointers, each npart long */
+    int32_t kernel;
+} pb_input;
+
+/* InterpolationCatalogConcise (InterpolationCatalog.jl:26-32), 0-based columns */
+typedef struct {
+    int32_t n_scalar;
+    const int32_t *scalar_cols;
+    const int32_t *scalar_shepard;   /* 0 for :rho / :ρ (InterpolationCatalog.jl:222-225) */
+    int32_t n_grad;
+    const int32_t *grad_cols;        /* -1 = density gradient */
+    int32_t n_div;
+    const int32_t *div_cols;         /* 3 per divergence */
+    int32_t n_curl;
+    const int32_t *curl_cols;        /* 3 per curl */
+} pb_catalog;
+
+/* Create a handle on CUDA device `device` (CUDAComputeBackend, CUDAExtDummy.jlh:12). */
+int32_t pb_create(pb_handle **out, int32_t device);
+void pb_destroy(pb_handle *h);
+/* Copy the last error message (NUL terminated) into buf; returns its full length. */
+int32_t pb_last_error(const pb_handle *h, char *buf, int64_t size);
+/* Launch on this stream (a cudaStream_t of the handle's device); NULL = the handle's own. */
+int32_t pb_set_stream(pb_handle *h, void *cuda_stream);
+/* Options: "timing" (record CUDA events around build/traversal), "sort_queries"
+   (Morton-order queries before traversal; schedule only), "block_size". */
+int32_t pb_set_option(pb_handle *h, const char *name, int64_t value);
+
+/* LinearBVH!(input, Val(3)) (InterpolationInput.jl:203-223): MortonEncoding
+   (MortonCode.jl:38-45), BinaryRadixTree (BinaryRadixTree.jl:81-132) and LinearBVH
+   (LinearBVH.jl:55-87), built on the device; the particle columns are kept on the device
+   in sorted order.  With PB_PERMUTE_CALLER the caller's x,y,z,m,h,rho,quant buffers are
+   permuted in place like the reference. */
+int32_t pb_linear_bvh(pb_handle *h, const pb_input *in, int32_t flags);
+
+/* MortonEncoding.codes/.order of the last build (MortonCode.jl:8-13); order is 0-based. */
+int32_t pb_export_encoding(pb_handle *h, uint64_t *codes, int64_t *order);
+/* BinaryRadixTree left/right/escape/parent (2n-1 each), LinearBVH node_aabb min/max
+   ([3][n-1] axis-major) and node_hmax (n-1) of the last build (LinearBVH.jl:20-26). */
+int32_t pb_export_tree(pb_handle *h, int32_t *left, int32_t *right, int32_t *escape, int32_t *parent,
+                       double *bmin, double *bmax, double *hmax, int32_t *root);
+
+/* LBVH_find_nearest_h / LBVH_find_nearest (LinearBVHQueries.jl:79-140), batched:
+   h_out[i] = smoothing length of the nearest leaf, idx_out[i] = its 0-based sorted leaf
+   index (either output may be NULL). */
+int32_t pb_find_nearest_h(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                          double *h_out, int64_t *idx_out);
+/* LBVH_query! (LinearBVHQueries.jl:183-211), batched in two steps: pb_query_count gives
+   counts[i]; pb_query_neighbors writes each query's accepted 0-based sorted leaf indices in
+   DFS order at pool[offsets[i] ...] and the nearest accepted leaf (-1 if none). */
+int32_t pb_query_count(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                       const double *radius, int64_t *counts);
+int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                           const double *radius, const int64_t *offsets, int64_t *pool, int64_t *nearest);
+
+/* Per-point kernel loop of PointSamples_interpolation on the last build
+   (Partia.jl/src/julia/KernelInterpolation/grid_interpolation/PointSamples_interpolation.jl:99-184):
+   LBVH_find_nearest_h + _general_quantity_interpolate_kernel (general_interpolation.jl:1-669).
+   out holds L = n_scalar + 3 n_grad + n_div + 3 n_curl pointers of npts doubles, in the
+   catalog's ordered_names order. */
+int32_t pb_interpolate_points(pb_handle *h, const pb_catalog *cat, int64_t npts, const double *qx,
+                              const double *qy, const double *qz, int32_t strategy, int32_t precision,
+                              double *const *out);
+
+/* Per-line kernel loop of LineSamples_interpolation on the last build (LineSamples_interpolation.jl:47-99,
+   line_integrated_scalar_interpolation.jl:123-166).  Only itpScatter is accepted (others:
+   PB_ERR_INVALID, the reference's ArgumentError).  Directions must be unit vectors. */
+int32_t pb_interpolate_lines(pb_handle *h, const pb_catalog *cat, int64_t nlines, const double *ox,
+                             const double *oy, const double *oz, const double *dx, const double *dy,
+                             const double *dz, int32_t strategy, int32_t precision, double *const *out);
+
+/* Partia.PointSamples_interpolation(::CUDAComputeBackend, grid, input, catalog, strategy)
+   (Partia.jl/ext/CUDAExt/KernelInterpolation/grid_interpolation/PointSamples_interpolation.jl:12-29):
+   build + interpolate in one call. */
+int32_t pb_point_samples_interpolation(pb_handle *h, const pb_input *in, const pb_catalog *cat, int64_t npts,
+                                       const double *qx, const double *qy, const double *qz, int32_t strategy,
+                                       int32_t precision, double *const *out, int32_t flags);
+
+/* Partia.LineSamples_interpolation(::CUDAComputeBackend, lines, input, catalog, itpScatter)
+   (Partia.jl/ext/CUDAExt/KernelInterpolation/grid_interpolation/LineSamples_interpolation.jl:11-34). */
+int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb_catalog *cat, int64_t nlines,
+                                      const double *ox, const double *oy, const double *oz, const double *dx,
+                                      const double *dy, const double *dz, int32_t strategy, int32_t precision,
+                                      double *const *out, int32_t flags);
+
+/* Diagnostics: kernels launched by this handle so far; build / traversal device time of
+   the last call in ms (needs option "timing"); traversal kernel launches of the last call. */
+int64_t pb_launch_count(const pb_handle *h);
+int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms, int64_t *interp_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARTIA_B200_H */
