@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark of the LBVH build + SPH grid interpolation path on B200.
+
+Default workload (the configuration the headline metric is quoted on): a seeded
+2^21-particle warped gas disc (M4 kernel) interpolated onto a cylindrical grid of 256
+log-spaced radii x 256 phi x 64 z (4,194,304 points) with the catalog rho, vx, vy, vz
+(scalars), grad rho, div v and curl v (L = 11 outputs), strategy itpSymmetric, kernel sums
+in FP32 with compensated accumulation (FP64 distance tests and pair offsets).
+
+One step = one pass of the hot path over the snapshot with inputs resident in HBM:
+LinearBVH! (quantise, encode, radix sort, dedupe, gather, topology, refit) followed by the
+fused nearest-h + symmetric traversal + kernel sums for every grid point.
+  value     grid points / s of the interpolation stage (build excluded; CUDA events on
+            the launching stream), summed over ranks (weak scaling: one snapshot per GPU)
+  build_ms  LBVH build time per step (CUDA events)
+  e2e       the same metric through the public API (PointSamples_interpolation) with
+            pinned host buffers: H2D of the particles and sample points, build,
+            interpolation, D2H of the outputs and of the in-place-permuted particle columns
+  roofline  algorithmic bytes of the reference algorithm's traversal events (per query:
+            24 B point + 8 B x L outputs; nearest pass 32 B per internal visit + 24 B per
+            leaf test; main pass 36 B per internal visit + 28 B per leaf test + (2+k) x 4 B
+            per accepted neighbour, k = quantity columns read) / traversal kernel time,
+            against the measured HBM copy bandwidth
+--impl reference runs the CPU oracle port (the restated reference algorithm, all host
+threads) on a bounded sample of the same workload.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "interp grid pts/s (LBVH build ms reported beside it)"
+UNIT = "grid pts/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
+    ap.add_argument("--particles", type=int, default=1 << 21)
+    ap.add_argument("--grid", default="256,256,64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--json-out", default=None)
+    return ap.parse_args()
+
+
+def workload(args, rank):
+    from distorteddustydiscanalysistoolkits_b200 import synthetic
+    import distorteddustydiscanalysistoolkits_b200 as pb
+    ns, nphi, nz = (int(v) for v in args.grid.split(","))
+    p = synthetic.disc(args.particles, seed=2 + rank)
+    grid = synthetic.log_cylindrical_grid(ns, nphi, nz)
+    flat = pb.flatten(pb.Cylindrical, grid)
+    cols = synthetic.C2_COLUMNS
+    cat = pb.InterpolationCatalog(cols, **synthetic.C2_CATALOG)
+    config = {"workload": "warped gas disc, %d particles (M4), cylindrical %dx%dx%d log-r grid, itpSymmetric, "
+                          "L=%d (rho,vx,vy,vz; grad rho; div v; curl v)" % (args.particles, ns, nphi, nz, cat.L),
+              "particles": args.particles, "grid_points": len(flat), "outputs": cat.L, "kernel": "M4_spline",
+              "strategy": "itpSymmetric", "precision": args.precision}
+    return p, flat, cols, cat, config
+
+
+def _max_over_ranks(vals, world):
+    if world == 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join("/tmp", "pb_clocks_%d_%d.csv" % (os.getpid(), gpu))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(stats, L, k_cols, s):
+    """Reference-algorithm bytes of one traversal launch over all queries (see module doc)."""
+    nv, nl, mv, ml, acc = (stats[:, i].astype(np.float64).sum() for i in range(5))
+    nq = stats.shape[0]
+    return nq * (24 + 8 * L) + 32 * nv + 24 * nl + 36 * mv + 28 * ml + acc * (2 + k_cols) * s
+
+
+def cpu_baseline(p, flat, cols, cat, seconds):
+    """Oracle port on the host cores: full build + a strided sample of the grid points."""
+    import oracle
+    threads = oracle.max_threads()
+    t0 = time.perf_counter()
+    o = oracle.OracleLBVH(p["x"], p["y"], p["z"], p["h"]).attach(p["m"], p["rho"], [p[c] for c in cols])
+    build_s = time.perf_counter() - t0
+    n = len(flat)
+    probe = 2048
+    idx = np.arange(0, n, max(n // probe, 1))[:probe]
+    t0 = time.perf_counter()
+    o.interp_points(cat.oracle_dict(), *(c[idx] for c in flat.coor), strategy="itpSymmetric")
+    per = (time.perf_counter() - t0) / len(idx)
+    budget = max(seconds - build_s, 2.0)
+    m = int(min(n, max(probe, budget / max(per, 1e-9))))
+    idx = np.arange(0, n, max(n // m, 1))[:m]
+    t0 = time.perf_counter()
+    o.interp_points(cat.oracle_dict(), *(c[idx] for c in flat.coor), strategy="itpSymmetric")
+    dt = time.perf_counter() - t0
+    return {"value": len(idx) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "oracle (C, OpenMP, FP64) on every %d-th grid point (%d of %d), after a full %d-particle "
+                      "LBVH build (%.0f ms)" % (n // len(idx), len(idx), n, len(p["x"]), build_s * 1e3),
+            "build_ms": build_s * 1e3}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle
+    import distorteddustydiscanalysistoolkits_b200 as pb  # noqa: F401  (catalog/grid host types only)
+    p, flat, cols, cat, config = workload(args, 0)
+    threads = oracle.max_threads()
+    t0 = time.perf_counter()
+    o = oracle.OracleLBVH(p["x"], p["y"], p["z"], p["h"]).attach(p["m"], p["rho"], [p[c] for c in cols])
+    build_ms = (time.perf_counter() - t0) * 1e3
+    n = len(flat)
+    # bounded sample per step: about 2 s of CPU work, a different strided subset each step
+    probe = np.arange(0, n, n // 1024)[:1024]
+    t0 = time.perf_counter()
+    o.interp_points(cat.oracle_dict(), *(c[probe] for c in flat.coor), strategy="itpSymmetric")
+    per = (time.perf_counter() - t0) / len(probe)
+    S = int(min(n, max(1024, 2.0 / max(per, 1e-9))))
+    stride = max(n // S, 1)
+    times = []
+    for step in range(args.warmup + args.steps):
+        idx = np.arange(step % stride, n, stride)[:S]
+        t0 = time.perf_counter()
+        o.interp_points(cat.oracle_dict(), *(c[idx] for c in flat.coor), strategy="itpSymmetric")
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.mean(times))
+    value = S / (ms / 1e3)
+    sample = "every %d-th grid point (%d of %d) per step; LBVH build of all %d particles once (%.0f ms)" % (
+        stride, S, n, len(p["x"]), build_ms)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded disc)",
+            "config": dict(config, precision="fp64"), "build_ms": build_ms,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference Julia code cannot run on this box (no Julia toolchain); this arm is the C "
+                    "restatement of the reference algorithm (oracle/), OpenMP over all host threads"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import distorteddustydiscanalysistoolkits_b200 as pb
+    from distorteddustydiscanalysistoolkits_b200 import _lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    p, flat, cols, cat, config = workload(args, rank)
+    prec = pb.FP32C if args.precision == "fp32c" else pb.FP64
+    npts = len(flat)
+    backend = pb.CUDAComputeBackend(local)
+    H = backend.handle
+    H.set_option("timing", 1)
+    stream = torch.cuda.current_stream()
+    H.set_stream(stream.cuda_stream)
+
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in p.items()}
+    q = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in flat.coor]
+    outs = [torch.empty(npts, dtype=torch.float64, device="cuda") for _ in range(cat.L)]
+    inp = pb.InterpolationInput(dev["x"], dev["y"], dev["z"], dev["m"], dev["h"], dev["rho"],
+                                tuple(dev[c] for c in cols), smoothed_kernel=pb.M4_spline)
+    import ctypes
+    cin, ccat = inp._c_struct(), cat._c_struct()
+    optrs = (ctypes.c_void_p * cat.L)(*[o.data_ptr() for o in outs])
+    qp = [c.data_ptr() for c in q]
+    pcode = _lib.PB_FP32C if prec == pb.FP32C else _lib.PB_FP64
+
+    def step():
+        rc = H.lib.pb_point_samples_interpolation(H.h, ctypes.byref(cin), ctypes.byref(ccat), npts, qp[0], qp[1],
+                                                  qp[2], pb.itpSymmetric.code, pcode, optrs, 0)
+        H.check(rc, "pb_point_samples_interpolation")
+        b, i, nl = H.timings()
+        return b, i
+
+    flush = torch.empty(L2_FLUSH_BYTES // 8, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        step()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches0 = H.launch_count()
+    builds, interps = [], []
+    for _ in range(args.steps):
+        flush.zero_()            # L2 flush between timed steps, outside the per-step events
+        b, i = step()
+        builds.append(b)
+        interps.append(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = H.launch_count() - launches0
+    clocks = sampler.stop()
+    build_ms, interp_ms = float(np.mean(builds)), float(np.mean(interps))
+    build_ms, interp_ms, step_ms = _max_over_ranks([build_ms, interp_ms, build_ms + interp_ms], world)
+    value = world * npts / (interp_ms / 1e3)
+
+    # roofline of the traversal kernel (one launch per step for this catalog)
+    lb = pb.LinearBVH(backend, args.particles)
+    stats = pb.traversal_stats(lb, [c.cpu().numpy() for c in q], pb.itpSymmetric)
+    s = 4 if prec == pb.FP32C else 8
+    alg_bytes = algorithmic_bytes(stats, cat.L, len(cols), s)
+    peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(REPO, "MEASURED_PEAKS.json")) else None
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = alg_bytes / (interp_ms / 1e3) / 1e9
+    traffic = None
+    prof = os.path.join(REPO, "profiles", "k_points_fp32c_symmetric_c2.json")
+    if os.path.exists(prof) and args.precision == "fp32c" and args.particles == (1 << 21):
+        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_points<Comp32,itpSymmetric>" if s == 4 else "k_points<Exact64,itpSymmetric>",
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
+                "events_per_query": {k: float(stats[:, i].mean()) for i, k in enumerate(
+                    ("nearest_internal", "nearest_leaf", "main_internal", "main_leaf", "accepted"))}}
+
+    # accuracy of the FP32-compensated fields against the FP64 path (bit-exact to the oracle)
+    accuracy = None
+    if prec == pb.FP32C and not args.no_accuracy:
+        ref = pb.interpolate_points(lb, cat, q, pb.itpSymmetric, pb.FP64)
+        got = pb.interpolate_points(lb, cat, q, pb.itpSymmetric, pb.FP32C)
+        accuracy = {}
+        for name, a, r in zip(cat.ordered_names, got, ref):
+            a, r = a.cpu().numpy(), r.cpu().numpy()
+            ok = ~np.isnan(r)
+            sc = np.max(np.abs(r[ok]))
+            err = np.abs(a[ok] - r[ok]) / sc
+            accuracy[name] = {"max_field_scaled": float(err.max()), "rms_field_scaled": float(np.sqrt(np.mean(err ** 2)))}
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        def pinned(a):
+            t = torch.empty(len(a), dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = a
+            return t.numpy()
+
+        hp = {k: pinned(v) for k, v in p.items()}
+        pristine = {k: v.copy() for k, v in hp.items()}
+        hq = [pinned(c) for c in flat.coor]
+        hout = [pinned(np.zeros(npts)) for _ in range(cat.L)]
+        grid = pb.PointSamples(np.zeros(npts), hq)
+        H.set_stream(None)
+        times = []
+        for k in range(args.warmup + args.steps):
+            for key in hp:
+                hp[key][:] = pristine[key]
+            inp_h = pb.InterpolationInput(hp["x"], hp["y"], hp["z"], hp["m"], hp["h"], hp["rho"],
+                                          tuple(hp[c] for c in cols), smoothed_kernel=pb.M4_spline)
+            t0 = time.perf_counter()
+            pb.PointSamples_interpolation(backend, grid, inp_h, cat, pb.itpSymmetric, precision=prec, out=hout)
+            dt = time.perf_counter() - t0
+            if k >= args.warmup:
+                times.append(dt)
+        e2e_s = _max_over_ranks([float(np.mean(times))], world)[0]
+        ncols_in = 6 + len(cols)
+        e2e = {"value": world * npts / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
+               "h2d_bytes_per_step": ncols_in * 8 * args.particles + 24 * npts,
+               "d2h_bytes_per_step": cat.L * 8 * npts + ncols_in * 8 * args.particles,
+               "path": "PointSamples_interpolation(CUDAComputeBackend) with pinned host arrays: H2D, build, "
+                       "interpolation, D2H of outputs and of the permuted particle columns"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(p, flat, cols, cat, args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32" if prec == pb.FP32C else "f64",
+                "data": "synthetic (seeded Philox disc, no dataset exists for this path)",
+                "config": dict(config, parallelism="replicas x%d (one snapshot per GPU)" % world,
+                               l2_flush="256 MiB write between timed steps, outside the step events"),
+                "build_ms": build_ms, "interp_ms": interp_ms,
+                "pts_per_s_with_build": world * npts / (step_ms / 1e3),
+                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clocks, "accuracy_fp32c_vs_fp64": accuracy}
+        txt = json.dumps(line)
+        print(txt, flush=True)
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                f.write(txt + "\n")
+    backend.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -14,6 +14,6 @@ from .interpolation import (C2_Wendland, C4_Wendland, C6_Wendland, CUDAComputeBa
                             StructuredGrid_interpolation, build_input, interpolate_lines, interpolate_points,
                             itpGather, itpScatter, itpSymmetric)
 from .neighbor import (LBVH_find_nearest, LBVH_find_nearest_h, LBVH_query, LinearBVH, LinearBVH_build,
-                       MortonEncoding, NeighborSelection)
+                       MortonEncoding, NeighborSelection, traversal_stats)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

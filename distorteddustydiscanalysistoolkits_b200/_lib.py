@@ -58,7 +58,7 @@ class PBCatalog(ctypes.Structure):
 
 
 EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set_option", "pb_linear_bvh",
-            "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors",
+            "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors", "pb_traversal_stats",
             "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
             "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings"]
 
@@ -87,6 +87,7 @@ def load():
         "pb_find_nearest_h": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
         "pb_query_count": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
         "pb_query_neighbors": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+        "pb_traversal_stats": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int32, _vp]),
         "pb_interpolate_points": (ctypes.c_int32, [_vp, P(PBCatalog), ctypes.c_int64, _vp, _vp, _vp,
                                                    ctypes.c_int32, ctypes.c_int32, P(_vp)]),
         "pb_interpolate_lines": (ctypes.c_int32, [_vp, P(PBCatalog), ctypes.c_int64] + [_vp] * 6 +

@@ -519,7 +519,7 @@ __device__ __forceinline__ int lcp(const uint64_t *__restrict__ c1, int64_t i, i
 }
 
 __global__ void k_karras(int64_t n, const uint64_t *__restrict__ codes, int *left, int *right, int *parent,
-                         int *escape)
+                         int *escape, int2 *child, int2 *range)
 {
     const uint64_t *c1 = codes - 1;
     const int64_t off = n - 1;
@@ -564,6 +564,8 @@ __global__ void k_karras(int64_t n, const uint64_t *__restrict__ codes, int *lef
         int64_t ri = (split + 1 == hi) ? hi + off : split + 1;
         left[i - 1] = (int)li;
         right[i - 1] = (int)ri;
+        child[i - 1] = make_int2((int)li, (int)ri);
+        range[i - 1] = make_int2((int)(lo - 1), (int)(hi - 1));   // 0-based sorted leaf range of the subtree
         parent[li - 1] = (int)i;
         parent[ri - 1] = (int)i;
         // internal escape (BinaryRadixTree.jl:245-260); adj[k] = lcp(k, k+1), adj[n] = +inf
@@ -663,7 +665,8 @@ cudaError_t launch_topology(Handle *H, int64_t n)
     cudaMemsetAsync(H->parent.p, 0, sizeof(int) * ntot, H->stream);
     cudaMemsetAsync(H->counters.p, 0, sizeof(unsigned) * (n - 1), H->stream);
     k_karras<<<grid_for(n - 1, 256), 256, 0, H->stream>>>(n, H->codes.as<uint64_t>(), H->left.as<int>(),
-                                                          H->right.as<int>(), H->parent.as<int>(), H->escape.as<int>());
+                                                          H->right.as<int>(), H->parent.as<int>(), H->escape.as<int>(),
+                                                          H->node_child.as<int2>(), H->node_range.as<int2>());
     k_refit<<<grid_for(n, 256, 1 << 30), 256, 0, H->stream>>>(
         n, H->parent.as<int>(), H->left.as<int>(), H->right.as<int>(), H->escape.as<int>(), H->leaf.as<double4>(),
         H->node.as<NodeF>(), H->node_hmax.as<float>(), H->bmin64.as<double>(), H->bmax64.as<double>(),

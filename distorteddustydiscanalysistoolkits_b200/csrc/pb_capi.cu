@@ -22,7 +22,7 @@ struct pb_handle {
 pb::Handle::~Handle()
 {
     DBuf *all[] = {&in_x, &in_y, &in_z, &in_h, &in_m, &in_rho, &codes, &codes_alt, &idx, &idx_alt, &scan_tmp,
-                   &scan_part, &hist, &bbox_part, &qparams, &status, &leaf, &leaf_escape, &node, &node_hmax, &left,
+                   &scan_part, &hist, &bbox_part, &qparams, &status, &leaf, &leaf_escape, &node, &node_hmax, &node_child, &node_range, &payload, &counter, &left,
                    &right, &escape, &parent, &bmin64, &bmax64, &hmax64, &counters, &m_s, &rho_s, &col_ptrs,
                    &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux};
     for (DBuf *b : all) b->release();
@@ -96,6 +96,8 @@ DevTree make_tree(Handle &H)
     T.leaf_escape = H.leaf_escape.as<int>();
     T.node = H.node.as<NodeF>();
     T.node_hmax = H.node_hmax.as<float>();
+    T.child = H.node_child.as<int2>();
+    T.range = H.node_range.as<int2>();
     T.m = H.m_s.as<double>();
     T.rho = H.rho_s.as<double>();
     T.kernel = H.kernel;
@@ -351,6 +353,8 @@ int do_build(Handle &H, const pb_input *in, int32_t flags)
     CK(H.leaf_escape.reserve(4 * n));
     CK(H.node.reserve(sizeof(NodeF) * nin));
     CK(H.node_hmax.reserve(4 * nin));
+    CK(H.node_child.reserve(8 * nin));
+    CK(H.node_range.reserve(8 * nin));
     CK(H.left.reserve(4 * nin));
     CK(H.right.reserve(4 * nin));
     CK(H.escape.reserve(4 * ntot));
@@ -687,6 +691,31 @@ int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const d
                     H.q_out.as<int64_t>()));
     if (!pool_dev && total > 0) CK(cudaMemcpyAsync(pool, dpool, 8 * total, cudaMemcpyDeviceToHost, H.stream));
     if (nearest) CK(cudaMemcpyAsync(nearest, H.q_out.p, 8 * npts, cudaMemcpyDefault, H.stream));
+    return check_status(H);
+}
+
+int32_t pb_traversal_stats(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                           int32_t strategy, int64_t *stats)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (strategy < 0 || strategy > 2) return fail(H, PB_ERR_INVALID, "unknown interpolation strategy");
+    if (npts <= 0) return npts == 0 ? PB_OK : fail(H, PB_ERR_INVALID, "negative npts");
+    if (!stats) return fail(H, PB_ERR_INVALID, "NULL stats");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dx, *dy, *dz;
+    int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
+    if (rc) return rc;
+    int64_t *ds = stats;
+    bool dev = is_device_ptr(stats);
+    if (!dev) {
+        CK(H.q_aux.reserve(40 * npts));
+        ds = H.q_aux.as<int64_t>();
+    }
+    CK(launch_stats(&H, make_tree(H), strategy, npts, dx, dy, dz, ds));
+    if (!dev) CK(cudaMemcpyAsync(stats, ds, 40 * npts, cudaMemcpyDeviceToHost, H.stream));
     return check_status(H);
 }
 

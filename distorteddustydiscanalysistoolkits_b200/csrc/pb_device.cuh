@@ -48,6 +48,8 @@ struct DevTree {
     const int *leaf_escape;
     const NodeF *node;
     const float *node_hmax;
+    const int2 *child;      // (left, right) unified ids of each internal node
+    const int2 *range;      // 0-based sorted leaf range [lo, hi] of each internal node's subtree
     const double *m;
     const double *rho;
     int kernel;

@@ -57,7 +57,9 @@ struct Handle {
     std::vector<DBuf> in_cols;
     DBuf codes, codes_alt, idx, idx_alt, scan_tmp, scan_part, hist;
     DBuf bbox_part, qparams, status;
-    DBuf leaf, leaf_escape, node, node_hmax;
+    DBuf leaf, leaf_escape, node, node_hmax, node_child, node_range;
+    DBuf payload;       // per-call FP32 particle payload of the FP32-compensated path
+    DBuf counter;       // work-queue counter of the warp-per-query kernels
     DBuf left, right, escape, parent;
     DBuf bmin64, bmax64, hmax64, counters;
     DBuf m_s, rho_s;
@@ -110,7 +112,8 @@ cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double
 cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
                          const double *qz, const double *radius, const int64_t *offsets, int64_t *counts,
                          int64_t *pool, int64_t *nearest);
-cudaError_t upload_line_tables();
+cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, const double *qx, const double *qy,
+                         const double *qz, int64_t *stats);
 
 inline int grid_for(int64_t n, int block, int cap = 148 * 32)
 {

@@ -1,5 +1,20 @@
-// pb_interp32.cu -- FP32-compensated point/line interpolation kernels (same neighbour
-// sets as the FP64 path; FP32 kernel sums with TwoSum compensation and offsets).
+// pb_interp32.cu -- FP32-compensated interpolation kernels.
+//
+// Same neighbour sets as the FP64 path: the nearest search, the node pruning and every
+// per-leaf acceptance test run in FP64 exactly as there, and accepted neighbours are
+// processed in the same DFS order.  Per pair, the kernel values and the accumulated terms
+// are FP32:
+//   * a per-call particle payload (built once per launch) holds 1/h_b, sigma h_b^-3,
+//     sigma h_b^-4, m_b/rho_b and every quantity column as a (hi, lo) float pair, so the
+//     pair needs no division and no FP64 column arithmetic;
+//   * kernel shapes are evaluated branch-free from their truncated-power forms
+//     (M4: 0.25 (2-q)_+^3 - (1-q)_+^3, ...), templated on the kernel type;
+//   * every quantity enters as an offset A_b - A_hat (A_hat = first accepted neighbour's
+//     value, as a double-float) so that gradient/divergence/curl F - A B does not cancel;
+//   * sums are accumulated per chunk of 4 accepted pairs in plain FP32 and each chunk sum
+//     is folded into a TwoSum-compensated accumulator.
+// The per-query arithmetic depends only on the query and the tree (chunks are counted over
+// the query's own accepted-neighbour sequence), never on the launch shape or schedule.
 #include "line_tables.h"
 #include "pb_internal.h"
 #include "pb_interp_impl.cuh"
@@ -8,17 +23,401 @@ namespace pb {
 
 __device__ const float g_line_inorm32[6][PB_LINE_NTAB] = PB_LINE_INORM_INIT;
 
+constexpr int CHUNK = 4;
+
+// ---- branch-free kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) ----
+template <int KT>
+__device__ __forceinline__ void shape(float q, float &f, float &df)
+{
+    if (KT == 0) {   // M4
+        float a = fmaxf(2.f - q, 0.f), b = fmaxf(1.f - q, 0.f);
+        f = 0.25f * a * a * a - b * b * b;
+        df = -0.75f * a * a + 3.f * b * b;
+    } else if (KT == 1) {   // M5
+        float a = fmaxf(2.5f - q, 0.f), b = fmaxf(1.5f - q, 0.f), c = fmaxf(0.5f - q, 0.f);
+        float a2 = a * a, b2 = b * b, c2 = c * c;
+        f = a2 * a2 - 5.f * b2 * b2 + 10.f * c2 * c2;
+        df = -4.f * a2 * a + 20.f * b2 * b - 40.f * c2 * c;
+    } else if (KT == 2) {   // M6
+        float a = fmaxf(3.f - q, 0.f), b = fmaxf(2.f - q, 0.f), c = fmaxf(1.f - q, 0.f);
+        float a4 = (a * a) * (a * a), b4 = (b * b) * (b * b), c4 = (c * c) * (c * c);
+        f = a4 * a - 6.f * b4 * b + 15.f * c4 * c;
+        df = -5.f * a4 + 30.f * b4 - 75.f * c4;
+    } else if (KT == 3) {   // C2
+        float t = fmaxf(1.f - 0.5f * q, 0.f);
+        float t3 = t * t * t;
+        f = t3 * t * (2.f * q + 1.f);
+        df = t3 * (2.f * t - (4.f * q + 2.f));
+    } else if (KT == 4) {   // C4
+        float t = fmaxf(1.f - 0.5f * q, 0.f);
+        float t5 = (t * t) * (t * t) * t;
+        f = t5 * t * ((35.f / 12.f) * q * q + 3.f * q + 1.f);
+        df = t5 * (t * ((35.f / 6.f) * q + 3.f) - ((35.f / 4.f) * q * q + 9.f * q + 3.f));
+    } else {   // C6
+        float t = fmaxf(1.f - 0.5f * q, 0.f);
+        float t7 = (t * t) * (t * t) * (t * t) * t;
+        f = t7 * t * (((4.f * q + 6.25f) * q + 4.f) * q + 1.f);
+        df = t7 * (t * ((12.f * q + 12.5f) * q + 4.f) - (((16.f * q + 25.f) * q + 16.f) * q + 4.f));
+    }
+}
+
+__device__ __forceinline__ float ldexp_norm3(int k)
+{
+    const float pi = 3.14159265358979f;
+    switch (k) {
+    case 0: return 1.f / pi;
+    case 1: return 0.05f / pi;
+    case 2: return 1.f / (120.f * pi);
+    case 3: return 21.f / (16.f * pi);
+    case 4: return 495.f / (256.f * pi);
+    default: return 1365.f / (512.f * pi);
+    }
+}
+
+// payload: record of stride float4s per sorted particle
+//   [0] = {1/h, sigma h^-3, sigma h^-4, m/rho}, then (hi, lo) pairs of the launch's columns
+__global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int stride)
+{
+    const float sig = ldexp_norm3(T.kernel);
+    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x) {
+        double h = T.leaf[b].w;
+        double ih = 1.0 / h;
+        float4 p0 = make_float4((float)ih, (float)(sig * ih * ih * ih), (float)(sig * ih * ih * ih * ih),
+                                (float)(T.m[b] / T.rho[b]));
+        float4 *rec = pay + b * stride;
+        rec[0] = p0;
+        float v[2 * MAXU];
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) {
+            double a = (u < C.nU) ? C.ucol[u][b] : 0.0;
+            float hi = (float)a;
+            v[2 * u] = hi;
+            v[2 * u + 1] = (float)(a - (double)hi);
+        }
+        for (int k = 1; k < stride; ++k) rec[k] = make_float4(v[4 * k - 4], v[4 * k - 3], v[4 * k - 2], v[4 * k - 1]);
+    }
+}
+
+struct Acc32 {
+    float pS1, pSA[MAXU], pB[3], pF[MAXG][3], pD[MAXD], pC[MAXC][3];
+    CSum S1, SA[MAXU], B[3], F[MAXG][3], D[MAXD], Cc[MAXC][3];
+    float hh[MAXU], hl[MAXU];
+    int cnt;
+    bool have;
+
+    __device__ __forceinline__ void zero_partials()
+    {
+        pS1 = 0.f;
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) pSA[u] = 0.f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pB[d] = 0.f;
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) pF[j][0] = pF[j][1] = pF[j][2] = 0.f;
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) pD[j] = 0.f;
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) pC[j][0] = pC[j][1] = pC[j][2] = 0.f;
+    }
+
+    __device__ __forceinline__ void init()
+    {
+        zero_partials();
+        S1.zero();
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) { SA[u].zero(); hh[u] = 0.f; hl[u] = 0.f; }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) B[d].zero();
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) { F[j][0].zero(); F[j][1].zero(); F[j][2].zero(); }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) D[j].zero();
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) { Cc[j][0].zero(); Cc[j][1].zero(); Cc[j][2].zero(); }
+        cnt = 0;
+        have = false;
+    }
+
+    __device__ __forceinline__ void flush(const DevCatalog &C, bool need_grad)
+    {
+        S1.add(pS1);
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u)
+            if (u < C.nU) SA[u].add(pSA[u]);
+        if (need_grad) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) B[d].add(pB[d]);
+#pragma unroll
+            for (int j = 0; j < MAXG; ++j)
+                if (j < C.n_grad) { F[j][0].add(pF[j][0]); F[j][1].add(pF[j][1]); F[j][2].add(pF[j][2]); }
+#pragma unroll
+            for (int j = 0; j < MAXD; ++j)
+                if (j < C.n_div) D[j].add(pD[j]);
+#pragma unroll
+            for (int j = 0; j < MAXC; ++j)
+                if (j < C.n_curl) { Cc[j][0].add(pC[j][0]); Cc[j][1].add(pC[j][1]); Cc[j][2].add(pC[j][2]); }
+        }
+        zero_partials();
+        cnt = 0;
+    }
+};
+
+struct Query32 {
+    float ih, cw, cg;   // 1/h_a, sigma h_a^-3, sigma h_a^-4
+};
+
+template <int STRAT, int KT>
+__device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
+                                       const float4 *__restrict__ pay, int stride, int64_t b, float dx, float dy,
+                                       float dz)
+{
+    const float4 *rec = pay + b * stride;
+    float4 p0 = __ldg(rec);
+    float r2 = dx * dx + dy * dy + dz * dz;
+    float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+    float r = r2 * rinv;
+    float W, G;
+    if (STRAT == SYMMETRIC) {
+        float fa, dfa, fb, dfb;
+        shape<KT>(r * Q.ih, fa, dfa);
+        shape<KT>(r * p0.x, fb, dfb);
+        W = 0.5f * (Q.cw * fa + p0.y * fb);
+        G = 0.5f * (Q.cg * dfa + p0.z * dfb) * rinv;
+    } else if (STRAT == GATHER) {
+        float f, df;
+        shape<KT>(r * Q.ih, f, df);
+        W = Q.cw * f;
+        G = Q.cg * df * rinv;
+    } else {
+        float f, df;
+        shape<KT>(r * p0.x, f, df);
+        W = p0.y * f;
+        G = p0.z * df * rinv;
+    }
+    float w = p0.w * W;
+    float a[MAXU];
+#pragma unroll
+    for (int k = 1; k <= (MAXU + 1) / 2; ++k) {
+        if (k < stride) {
+            float4 c = __ldg(rec + k);
+            a[2 * k - 2] = (c.x - A.hh[2 * k - 2]) + (c.y - A.hl[2 * k - 2]);
+            if (2 * k - 1 < MAXU) a[2 * k - 1] = (c.z - A.hh[2 * k - 1]) + (c.w - A.hl[2 * k - 1]);
+        } else {
+            a[2 * k - 2] = 0.f;
+            if (2 * k - 1 < MAXU) a[2 * k - 1] = 0.f;
+        }
+    }
+    A.pS1 += w;
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) A.pSA[u] += a[u] * w;
+    if (need_grad) {
+        float gq = p0.w * G;
+        float gx = gq * dx, gy = gq * dy, gz = gq * dz;
+        A.pB[0] += gx; A.pB[1] += gy; A.pB[2] += gz;
+#pragma unroll
+        for (int j = 0; j < MAXG; ++j) {
+            if (j < C.n_grad) {
+                float av = pick<MAXU>(a, C.g_u[j]);
+                A.pF[j][0] += gx * av; A.pF[j][1] += gy * av; A.pF[j][2] += gz * av;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXD; ++j) {
+            if (j < C.n_div) {
+                float ax = pick<MAXU>(a, C.d_u[j][0]), ay = pick<MAXU>(a, C.d_u[j][1]), az = pick<MAXU>(a, C.d_u[j][2]);
+                A.pD[j] += gx * ax + gy * ay + gz * az;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXC; ++j) {
+            if (j < C.n_curl) {
+                float ax = pick<MAXU>(a, C.c_u[j][0]), ay = pick<MAXU>(a, C.c_u[j][1]), az = pick<MAXU>(a, C.c_u[j][2]);
+                A.pC[j][0] += ay * gz - az * gy;
+                A.pC[j][1] += az * gx - ax * gz;
+                A.pC[j][2] += ax * gy - ay * gx;
+            }
+        }
+    }
+    if (++A.cnt == CHUNK) A.flush(C, need_grad);
+}
+
+__device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, const DevCatalog &C, int64_t qi)
+{
+    int l = 0;
+    double S = v[0];
+    if (S == 0.0) {
+        for (int o = 0; o < C.L; ++o) C.out[o][qi] = __longlong_as_double(0x7ff8000000000000LL);
+        return;
+    }
+    double abar[MAXU], ah[MAXU], sav[MAXU];
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) {
+        sav[u] = v[1 + u];
+        abar[u] = sav[u] / S;
+        ah[u] = (double)A.hh[u] + (double)A.hl[u];
+    }
+    const double B[3] = {v[5], v[6], v[7]};
+#pragma unroll
+    for (int j = 0; j < MAXS; ++j) {
+        if (j < C.n_scalar) {
+            int u = C.s_u[j];
+            double h0 = pick<MAXU>(ah, u);
+            C.out[l++][qi] = C.s_shep[j] ? h0 + pick<MAXU>(abar, u) : h0 * S + pick<MAXU>(sav, u);
+        }
+    }
+    if (C.n_grad > 0) {
+        double a = pick<MAXU>(abar, C.g_u[0]);
+        C.out[l++][qi] = v[8] - a * B[0];
+        C.out[l++][qi] = v[9] - a * B[1];
+        C.out[l++][qi] = v[10] - a * B[2];
+    }
+    if (C.n_div > 0) {
+        double ax = pick<MAXU>(abar, C.d_u[0][0]), ay = pick<MAXU>(abar, C.d_u[0][1]), az = pick<MAXU>(abar, C.d_u[0][2]);
+        C.out[l++][qi] = v[11] - (ax * B[0] + ay * B[1] + az * B[2]);
+    }
+    if (C.n_curl > 0) {
+        double ax = pick<MAXU>(abar, C.c_u[0][0]), ay = pick<MAXU>(abar, C.c_u[0][1]), az = pick<MAXU>(abar, C.c_u[0][2]);
+        double bx = ay * B[2] - az * B[1];
+        double by = az * B[0] - ax * B[2];
+        double bz = ax * B[1] - ay * B[0];
+        C.out[l++][qi] = -(v[12] - bx);
+        C.out[l++][qi] = -(v[13] - by);
+        C.out[l++][qi] = -(v[14] - bz);
+    }
+}
+
+template <int STRAT, int KT>
+__global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
+                                                   int64_t nq, const double *__restrict__ qx,
+                                                   const double *__restrict__ qy, const double *__restrict__ qz,
+                                                   const uint32_t *__restrict__ perm, unsigned long long *counter)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t n = T.n;
+    const double K = kernel_valid(KT);
+    const float sig = ldexp_norm3(KT);
+    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
+    for (;;) {
+        int64_t j = next_query(counter, lane);
+        if (j >= nq) break;
+        int64_t qi = perm ? (int64_t)__ldg(perm + j) : j;
+        if (qi >= nq) continue;
+        double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        double ha = 0.0;
+        Query32 Q{0.f, 0.f, 0.f};
+        if (STRAT != SCATTER) {
+            int64_t b = nearest_leaf(T, px, py, pz);
+            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
+            float ih = (float)(1.0 / ha);
+            Q.ih = ih;
+            Q.cw = sig * ih * ih * ih;
+            Q.cg = Q.cw * ih;
+        }
+        double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
+        Acc32 A;
+        A.init();
+        Slots S{0, -1};
+        auto proc = [&](int fill) {
+            if (!A.have) {
+                int64_t b0 = __shfl_sync(0xffffffffu, S.mine, 0);
+                const float4 *rec = pay + b0 * stride;
+#pragma unroll
+                for (int k = 1; k <= (MAXU + 1) / 2; ++k) {
+                    if (k < stride) {
+                        float4 c = __ldg(rec + k);
+                        A.hh[2 * k - 2] = c.x; A.hl[2 * k - 2] = c.y;
+                        if (2 * k - 1 < MAXU) { A.hh[2 * k - 1] = c.z; A.hl[2 * k - 1] = c.w; }
+                    }
+                }
+                A.have = true;
+            }
+            if (S.mine >= 0) {
+                double4 L = ldg4(T.leaf + S.mine);
+                pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, S.mine, (float)(px - L.x), (float)(py - L.y),
+                                  (float)(pz - L.z));
+            }
+        };
+        if (T.root == 0) {
+            double4 L;
+            double d2;
+            if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2)) deal(S, lane, 0, 0, proc);
+        } else {
+            Walk w{T.root, 1, 0, 0, 4 * n + 64};
+            int64_t lo, hi;
+            while (next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) deal(S, lane, lo, hi, proc);
+        }
+        if (S.fill > 0) proc(S.fill);
+        A.flush(C, need_grad);
+        // fixed-tree FP64 reduction of the 32 lane sums
+        double v[15];
+        v[0] = A.S1.val();
+#pragma unroll
+        for (int u = 0; u < MAXU; ++u) v[1 + u] = A.SA[u].val();
+        v[5] = A.B[0].val(); v[6] = A.B[1].val(); v[7] = A.B[2].val();
+        v[8] = A.F[0][0].val(); v[9] = A.F[0][1].val(); v[10] = A.F[0][2].val();
+        v[11] = A.D[0].val();
+        v[12] = A.Cc[0][0].val(); v[13] = A.Cc[0][1].val(); v[14] = A.Cc[0][2].val();
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+            for (int a = 0; a < 15; ++a) v[a] += __shfl_down_sync(0xffffffffu, v[a], off);
+        }
+        if (lane == 0) finalize32w(v, A, C, qi);
+    }
+}
+
+static int persistent_grid(const void *kern, int bs)
+{
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, bs, 0);
+    return sms * (per > 0 ? per : 1);
+}
+
+template <int STRAT, int KT>
+static void launch_one(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride, int64_t nq,
+                       const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                       unsigned long long *ctr)
+{
+    const int bs = 128;
+    k_points32w<STRAT, KT><<<persistent_grid((const void *)k_points32w<STRAT, KT>, bs), bs, 0, H->stream>>>(
+        T, C, pay, stride, nq, qx, qy, qz, perm, ctr);
+}
+
+template <int STRAT>
+static void launch_kt(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride, int64_t nq,
+                      const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                      unsigned long long *ctr)
+{
+    switch (T.kernel) {
+    case 0: launch_one<STRAT, 0>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case 1: launch_one<STRAT, 1>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case 2: launch_one<STRAT, 2>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case 3: launch_one<STRAT, 3>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case 4: launch_one<STRAT, 4>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    default: launch_one<STRAT, 5>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    }
+}
+
 cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
                                const double *qx, const double *qy, const double *qz, const uint32_t *perm)
 {
-    int bs = 128;
-    int grid = grid_for(nq, bs, 1 << 30);
+    int stride = 1 + (C.nU + 1) / 2;
+    cudaError_t e = H->payload.reserve(sizeof(float4) * stride * T.n);
+    if (e) return e;
+    e = H->counter.reserve(sizeof(unsigned long long));
+    if (e) return e;
+    float4 *pay = H->payload.as<float4>();
+    unsigned long long *ctr = H->counter.as<unsigned long long>();
+    k_payload<<<grid_for(T.n, 256), 256, 0, H->stream>>>(T.n, T, C, pay, stride);
+    cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), H->stream);
     switch (strategy) {
-    case GATHER: k_points<Comp32, GATHER><<<grid, bs, 0, H->stream>>>(T, C, nq, qx, qy, qz, perm); break;
-    case SCATTER: k_points<Comp32, SCATTER><<<grid, bs, 0, H->stream>>>(T, C, nq, qx, qy, qz, perm); break;
-    default: k_points<Comp32, SYMMETRIC><<<grid, bs, 0, H->stream>>>(T, C, nq, qx, qy, qz, perm); break;
+    case GATHER: launch_kt<GATHER>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case SCATTER: launch_kt<SCATTER>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    default: launch_kt<SYMMETRIC>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
     }
-    H->launches += 1;
+    H->launches += 2;
     return cudaGetLastError();
 }
 

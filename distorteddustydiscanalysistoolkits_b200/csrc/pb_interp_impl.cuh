@@ -31,41 +31,6 @@ __device__ __forceinline__ T pick(const T (&a)[N], int i)
 
 __device__ __forceinline__ void flag(int *status, int bit) { atomicOr(status, bit); }
 
-// LBVH_find_nearest_h (LinearBVHQueries.jl:118-140): min squared distance, first in DFS order
-// (= smallest sorted leaf index) among ties.
-__device__ __forceinline__ int64_t nearest_leaf(const DevTree &T, double px, double py, double pz)
-{
-    double best = INFINITY;
-    int64_t bi = -1;
-    const int64_t n = T.n;
-    if (T.root == 0) {
-        double d2 = d2_point(px, py, pz, ldg4(T.leaf));
-        if (d2 < best) bi = 0;
-        return bi;
-    }
-    int node = T.root;
-    int64_t guard = 0, limit = 4 * n + 64;
-    while (node != 0) {
-        if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
-        if (node >= n) {
-            int64_t b = node - n;
-            double4 L = ldg4(T.leaf + b);
-            int esc = __ldg(T.leaf_escape + b);
-            double d2 = d2_point(px, py, pz, L);
-            if (d2 < best) { best = d2; bi = b; }
-            node = esc;
-        } else {
-            const float4 *np = reinterpret_cast<const float4 *>(T.node + (node - 1));
-            float4 a = __ldg(np), c = __ldg(np + 1);
-            NodeF nd;
-            nd.lox = a.x; nd.loy = a.y; nd.loz = a.z; nd.left = __float_as_int(a.w);
-            nd.hix = c.x; nd.hiy = c.y; nd.hiz = c.z; nd.escape = __float_as_int(c.w);
-            node = (d2_box(px, py, pz, nd) > best) ? nd.escape : nd.left;
-        }
-    }
-    return bi;
-}
-
 __device__ __forceinline__ NodeF load_node(const NodeF *p)
 {
     const float4 *q = reinterpret_cast<const float4 *>(p);
@@ -74,6 +39,236 @@ __device__ __forceinline__ NodeF load_node(const NodeF *p)
     nd.lox = a.x; nd.loy = a.y; nd.loz = a.z; nd.left = __float_as_int(a.w);
     nd.hix = c.x; nd.hiy = c.y; nd.hiz = c.z; nd.escape = __float_as_int(c.w);
     return nd;
+}
+
+// LBVH_find_nearest_h (LinearBVHQueries.jl:118-140).  The reference walks the tree in DFS
+// order with a shrinking radius and keeps the first strictly closer leaf, i.e. it returns
+// the minimum squared distance and, among equal distances, the smallest sorted leaf index.
+// This search visits the nearer child first (explicit stack) and applies exactly that
+// rule, so it returns the same leaf while visiting far fewer nodes.  Boxes are the FP32
+// outward-rounded ones (never farther than any leaf inside), and a subtree is skipped only
+// when its box distance is strictly greater than the best distance.
+constexpr int NN_STACK = 64;
+
+__device__ __forceinline__ double child_dist(const DevTree &T, int id, double px, double py, double pz,
+                                             double &best, int64_t &bi)
+{
+    const int64_t n = T.n;
+    if (id >= n) {
+        int64_t b = id - n;
+        double d2 = d2_point(px, py, pz, ldg4(T.leaf + b));
+        if (d2 < best || (d2 == best && b < bi)) { best = d2; bi = b; }
+        return INFINITY;   // a leaf needs no further visit
+    }
+    return d2_box(px, py, pz, load_node(T.node + (id - 1)));
+}
+
+__device__ __forceinline__ int64_t nearest_leaf(const DevTree &T, double px, double py, double pz)
+{
+    double best = INFINITY;
+    int64_t bi = -1;
+    if (T.root == 0) {
+        double d2 = d2_point(px, py, pz, ldg4(T.leaf));
+        return d2 < best ? 0 : -1;
+    }
+    int sn[NN_STACK];
+    double sd[NN_STACK];
+    int sp = 0;
+    int node = T.root;
+    int64_t guard = 0, limit = 4 * T.n + 64;
+    for (;;) {
+        if (++guard > limit) { atomicOr(T.status, ST_TRAVERSAL); break; }
+        int2 ch = __ldg(T.child + (node - 1));
+        double dl = child_dist(T, ch.x, px, py, pz, best, bi);
+        double dr = child_dist(T, ch.y, px, py, pz, best, bi);
+        bool vl = dl <= best, vr = dr <= best;
+        if (vl && vr) {
+            bool lf = dl <= dr;
+            int far = lf ? ch.y : ch.x;
+            double fd = lf ? dr : dl;
+            if (sp < NN_STACK) { sn[sp] = far; sd[sp] = fd; ++sp; }
+            else { atomicOr(T.status, ST_TRAVERSAL); }
+            node = lf ? ch.x : ch.y;
+            continue;
+        }
+        if (vl) { node = ch.x; continue; }
+        if (vr) { node = ch.y; continue; }
+        node = 0;
+        while (sp > 0) {
+            --sp;
+            if (sd[sp] <= best) { node = sn[sp]; break; }
+        }
+        if (node == 0) break;
+    }
+    return bi;
+}
+
+// Largest squared distance from the point to any point of the (outward-rounded) box,
+// with the rounding sequence of d2_point: every leaf inside has d2_point <= this value.
+__device__ __forceinline__ double far_d2_box(double px, double py, double pz, const NodeF &nd)
+{
+    double ax = fmax(fabs(__dsub_rn(px, (double)nd.lox)), fabs(__dsub_rn(px, (double)nd.hix)));
+    double ay = fmax(fabs(__dsub_rn(py, (double)nd.loy)), fabs(__dsub_rn(py, (double)nd.hiy)));
+    double az = fmax(fabs(__dsub_rn(pz, (double)nd.loz)), fabs(__dsub_rn(pz, (double)nd.hiz)));
+    double s = __dmul_rn(ax, ax);
+    s = __dadd_rn(s, __dmul_rn(ay, ay));
+    s = __dadd_rn(s, __dmul_rn(az, az));
+    return s;
+}
+
+
+// --------------------------------------------------------------------------------------
+// DFS walker of the main pass ("while-while" form): each call advances the stackless
+// left/escape traversal (LinearBVHTraversalMacros.jl:135-371) until the next accepted leaf
+// and returns it, so all lanes of a warp evaluate their pair terms together.  A subtree
+// lying entirely inside the query's radius is turned into a cursor over its contiguous
+// sorted-leaf range, which is exactly the DFS order of its leaves.  The sequence of
+// accepted leaves is therefore the reference's.
+struct Walk {
+    int node;
+    int64_t cur, end, guard, limit;
+};
+
+template <int STRAT>
+__device__ __forceinline__ int64_t next_accepted(const DevTree &T, Walk &w, double px, double py, double pz,
+                                                 double K, double r2a, double4 &L, double &d2)
+{
+    const int64_t n = T.n;
+    for (;;) {
+        if (w.cur <= w.end) {
+            int64_t b = w.cur++;
+            L = ldg4(T.leaf + b);
+            d2 = d2_point(px, py, pz, L);
+            return b;
+        }
+        if (w.node == 0) return -1;
+        if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.node = 0; return -1; }
+        const int node = w.node;
+        if (node >= n) {
+            int64_t b = node - n;
+            L = ldg4(T.leaf + b);
+            w.node = __ldg(T.leaf_escape + b);
+            double r2;
+            if (STRAT == GATHER) r2 = r2a;
+            else {
+                double r = __dmul_rn(K, L.w);
+                double rr = __dmul_rn(r, r);
+                r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+            }
+            d2 = d2_point(px, py, pz, L);
+            if (d2 <= r2) return b;
+            continue;
+        }
+        NodeF nd = load_node(T.node + (node - 1));
+        double r2;
+        if (STRAT == GATHER) r2 = r2a;
+        else {
+            double r = __dmul_rn(K, (double)__ldg(T.node_hmax + (node - 1)));
+            double rr = __dmul_rn(r, r);
+            r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+        }
+        if (d2_box(px, py, pz, nd) > r2) { w.node = nd.escape; continue; }
+        if (STRAT != SCATTER && far_d2_box(px, py, pz, nd) <= r2a) {
+            int2 rg = __ldg(T.range + (node - 1));
+            w.cur = rg.x;
+            w.end = rg.y;
+            w.node = nd.escape;
+            continue;
+        }
+        w.node = nd.left;
+    }
+}
+
+// Warp-uniform form of the same walk for the warp-per-query kernels: returns the next
+// accepted item in DFS order, either a single leaf (lo == hi) or the whole contiguous leaf
+// range of a subtree that lies inside the query radius.
+template <int STRAT>
+__device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, double py, double pz, double K,
+                                          double r2a, int64_t &lo, int64_t &hi)
+{
+    const int64_t n = T.n;
+    for (;;) {
+        if (w.node == 0) return false;
+        if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.node = 0; return false; }
+        const int node = w.node;
+        if (node >= n) {
+            int64_t b = node - n;
+            double4 L = ldg4(T.leaf + b);
+            w.node = __ldg(T.leaf_escape + b);
+            double r2;
+            if (STRAT == GATHER) r2 = r2a;
+            else {
+                double r = __dmul_rn(K, L.w);
+                double rr = __dmul_rn(r, r);
+                r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+            }
+            if (d2_point(px, py, pz, L) <= r2) { lo = hi = b; return true; }
+            continue;
+        }
+        NodeF nd = load_node(T.node + (node - 1));
+        double r2;
+        if (STRAT == GATHER) r2 = r2a;
+        else {
+            double r = __dmul_rn(K, (double)__ldg(T.node_hmax + (node - 1)));
+            double rr = __dmul_rn(r, r);
+            r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+        }
+        if (d2_box(px, py, pz, nd) > r2) { w.node = nd.escape; continue; }
+        if (STRAT != SCATTER && far_d2_box(px, py, pz, nd) <= r2a) {
+            int2 rg = __ldg(T.range + (node - 1));
+            lo = rg.x;
+            hi = rg.y;
+            w.node = nd.escape;
+            return true;
+        }
+        w.node = nd.left;
+    }
+}
+
+// Slot filler shared by the warp-per-query kernels: accepted leaves, in DFS order, are
+// dealt to the 32 lanes (the k-th accepted leaf goes to lane k mod 32); PROC(fill) is
+// called whenever 32 slots are full and once more for the remainder.
+struct Slots {
+    int fill;
+    int64_t mine;   // this lane's leaf in the current batch (-1 if none)
+};
+
+template <typename PROC>
+__device__ __forceinline__ void deal(Slots &S, int lane, int64_t lo, int64_t hi, PROC &proc)
+{
+    while (lo <= hi) {
+        int64_t t = hi - lo + 1;
+        int room = 32 - S.fill;
+        if (t > room) t = room;
+        if (lane >= S.fill && lane < S.fill + (int)t) S.mine = lo + (lane - S.fill);
+        S.fill += (int)t;
+        lo += t;
+        if (S.fill == 32) {
+            proc(32);
+            S.fill = 0;
+            S.mine = -1;
+        }
+    }
+}
+
+// query scheduling: warps take queries in the given order from a global counter
+__device__ __forceinline__ int64_t next_query(unsigned long long *counter, int lane)
+{
+    unsigned long long q = 0;
+    if (lane == 0) q = atomicAdd(counter, 1ULL);
+    return (int64_t)__shfl_sync(0xffffffffu, q, 0);
+}
+
+// the n == 1 tree has no internal node: its single leaf is tested directly
+template <int STRAT>
+__device__ __forceinline__ bool single_leaf_accepted(const DevTree &T, double px, double py, double pz, double K,
+                                                     double r2a, double4 &L, double &d2)
+{
+    L = ldg4(T.leaf);
+    double r = __dmul_rn(K, L.w), rr = __dmul_rn(r, r);
+    double r2 = STRAT == GATHER ? r2a : (STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr));
+    d2 = d2_point(px, py, pz, L);
+    return d2 <= r2;
 }
 
 // --------------------------------------------------------------------------------------
@@ -393,43 +588,16 @@ __global__ void __launch_bounds__(128) k_points(DevTree T, DevCatalog C, int64_t
         double r2a = __dmul_rn(ra, ra);
         ACC<STRAT> acc;
         acc.init();
+        double4 L;
+        double d2;
         if (T.root == 0) {
-            double4 L = ldg4(T.leaf);
-            double rr = __dmul_rn(__dmul_rn(K, L.w), __dmul_rn(K, L.w));
-            double r2 = STRAT == GATHER ? r2a : (STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr));
-            double d2 = d2_point(px, py, pz, L);
-            if (d2 <= r2) acc.add(T, C, need_grad, px, py, pz, L, 0, d2, ha, L.w);
+            if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2))
+                acc.add(T, C, need_grad, px, py, pz, L, 0, d2, ha, L.w);
         } else {
-            int node = T.root;
-            int64_t guard = 0, limit = 4 * n + 64;
-            while (node != 0) {
-                if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
-                if (node >= n) {
-                    int64_t b = node - n;
-                    double4 L = ldg4(T.leaf + b);
-                    int esc = __ldg(T.leaf_escape + b);
-                    double r2;
-                    if (STRAT == GATHER) r2 = r2a;
-                    else {
-                        double r = __dmul_rn(K, L.w);
-                        double rr = __dmul_rn(r, r);
-                        r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
-                    }
-                    double d2 = d2_point(px, py, pz, L);
-                    if (d2 <= r2) acc.add(T, C, need_grad, px, py, pz, L, b, d2, ha, L.w);
-                    node = esc;
-                } else {
-                    NodeF nd = load_node(T.node + (node - 1));
-                    double r2;
-                    if (STRAT == GATHER) r2 = r2a;
-                    else {
-                        double r = __dmul_rn(K, (double)__ldg(T.node_hmax + (node - 1)));
-                        double rr = __dmul_rn(r, r);
-                        r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
-                    }
-                    node = (d2_box(px, py, pz, nd) > r2) ? nd.escape : nd.left;
-                }
-            }
+            Walk w{T.root, 1, 0, 0, 4 * n + 64};
+            int64_t b;
+            while ((b = next_accepted<STRAT>(T, w, px, py, pz, K, r2a, L, d2)) >= 0)
+                acc.add(T, C, need_grad, px, py, pz, L, b, d2, ha, L.w);
         }
         acc.finalize(C, qi);
     }

@@ -61,6 +61,102 @@ __global__ void k_query(DevTree T, int64_t nq, const double *__restrict__ qx, co
     }
 }
 
+// Event counts of the reference algorithm itself (leaf size 1, Karras tree, left-first DFS,
+// FP64 boxes and the reference's pruning tests, LinearBVHTraversalMacros.jl:26-371): per
+// query [nearest-pass internal visits, nearest-pass leaf tests, main-pass internal visits,
+// main-pass leaf tests, accepted neighbours].  Used for the algorithmic-bytes roofline model
+// and as exact per-query work labels.
+struct Tree64 {
+    const double *bmin, *bmax, *hmax;
+};
+
+__device__ __forceinline__ double d2_box64(const Tree64 &B, int64_t nin, int64_t i0, double px, double py, double pz)
+{
+    double p[3] = {px, py, pz};
+    double s = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double a = B.bmin[d * nin + i0], b = B.bmax[d * nin + i0];
+        double t = p[d] < a ? __dsub_rn(a, p[d]) : (p[d] > b ? __dsub_rn(p[d], b) : 0.0);
+        s = __dadd_rn(s, __dmul_rn(t, t));
+    }
+    return s;
+}
+
+__global__ void k_stats(DevTree T, Tree64 B, int strategy, int64_t nq, const double *__restrict__ qx,
+                        const double *__restrict__ qy, const double *__restrict__ qz, int64_t *stats)
+{
+    const int64_t n = T.n, nin = n - 1;
+    const double K = kernel_valid(T.kernel);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x) {
+        double px = qx[i], py = qy[i], pz = qz[i];
+        int64_t nv = 0, nl = 0, mv = 0, ml = 0, acc = 0;
+        int64_t guard, limit = 4 * n + 64;
+        double ha = 0.0;
+        if (strategy != SCATTER) {
+            double best = INFINITY;
+            int64_t bi = -1;
+            if (T.root == 0) {
+                double d2 = d2_point(px, py, pz, ldg4(T.leaf));
+                ++nl;
+                if (d2 < best) bi = 0;
+            } else {
+                int node = T.root;
+                guard = 0;
+                while (node != 0) {
+                    if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
+                    if (node >= n) {
+                        int64_t b = node - n;
+                        double d2 = d2_point(px, py, pz, ldg4(T.leaf + b));
+                        ++nl;
+                        if (d2 < best) { best = d2; bi = b; }
+                        node = __ldg(T.leaf_escape + b);
+                    } else {
+                        ++nv;
+                        NodeF nd = load_node(T.node + (node - 1));
+                        node = (d2_box64(B, nin, node - 1, px, py, pz) > best) ? nd.escape : nd.left;
+                    }
+                }
+            }
+            ha = bi < 0 ? __longlong_as_double(0x7ff8000000000000LL) : T.leaf[bi].w;
+        }
+        double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
+        int node = T.root;
+        int64_t bi = 0;
+        bool brute = (node == 0);
+        guard = 0;
+        while (brute ? (bi < n) : (node != 0)) {
+            if (++guard > limit) { flag(T.status, ST_TRAVERSAL); break; }
+            if (brute || node >= n) {
+                int64_t b = brute ? bi++ : (int64_t)(node - n);
+                double4 L = ldg4(T.leaf + b);
+                double r = __dmul_rn(K, L.w), rr = __dmul_rn(r, r);
+                double r2 = strategy == GATHER ? r2a : (strategy == SCATTER ? rr : (r2a > rr ? r2a : rr));
+                ++ml;
+                if (d2_point(px, py, pz, L) <= r2) ++acc;
+                if (!brute) node = __ldg(T.leaf_escape + b);
+            } else {
+                ++mv;
+                NodeF nd = load_node(T.node + (node - 1));
+                double r = __dmul_rn(K, B.hmax[node - 1]), rr = __dmul_rn(r, r);
+                double r2 = strategy == GATHER ? r2a : (strategy == SCATTER ? rr : (r2a > rr ? r2a : rr));
+                node = (d2_box64(B, nin, node - 1, px, py, pz) > r2) ? nd.escape : nd.left;
+            }
+        }
+        int64_t *s = stats + 5 * i;
+        s[0] = nv; s[1] = nl; s[2] = mv; s[3] = ml; s[4] = acc;
+    }
+}
+
+cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, const double *qx, const double *qy,
+                         const double *qz, int64_t *stats)
+{
+    Tree64 B{H->bmin64.as<double>(), H->bmax64.as<double>(), H->hmax64.as<double>()};
+    k_stats<<<grid_for(nq, 128, 1 << 30), 128, 0, H->stream>>>(T, B, strategy, nq, qx, qy, qz, stats);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
                            const double *qz, double *h_out, int64_t *idx_out)
 {

@@ -289,17 +289,20 @@ def _strategy(s):
     raise ArgumentError("unknown interpolation strategy %r" % (s,))
 
 
-def PointSamples_interpolation(backend, grid_template, input, catalog, itp_strategy=itpSymmetric, precision=FP64):
+def PointSamples_interpolation(backend, grid_template, input, catalog, itp_strategy=itpSymmetric, precision=FP64,
+                               out=None):
     """Build the LBVH of ``input`` (permuting it in place) and interpolate the catalog at every
     point of ``grid_template``.  Returns a GridBundle of PointSamples sharing the template's
-    coordinates, one per catalog.ordered_names entry."""
+    coordinates, one per catalog.ordered_names entry (written into ``out`` when given)."""
     if not isinstance(backend, CUDAComputeBackend):
         raise ArgumentError("backend must be a CUDAComputeBackend")
     if not isinstance(grid_template, PointSamples):
         raise ArgumentError("grid_template must be PointSamples")
     H = backend.handle
     n = len(grid_template)
-    outs = _out_arrays(n, catalog.L)
+    outs = out if out is not None else _out_arrays(n, catalog.L)
+    if len(outs) != catalog.L:
+        raise DimensionMismatch("out must hold %d arrays" % catalog.L)
     cin, ccat = input._c_struct(), catalog._c_struct()
     optrs = _ptr_array(outs)
     qx, qy, qz = grid_template.coor

@@ -118,6 +118,18 @@ def LBVH_find_nearest(lbvh, points):
     return idx
 
 
+def traversal_stats(lbvh, points, itp_strategy):
+    """Per-point event counts of the reference traversal (nearest internal visits, nearest leaf
+    tests, main internal visits, main leaf tests, accepted neighbours) as an (N, 5) int64 array."""
+    qx, qy, qz = _pts(points)
+    n = len(qx)
+    st = np.empty((n, 5), np.int64)
+    H = lbvh.handle
+    H.check(H.lib.pb_traversal_stats(H.h, n, ptr(qx), ptr(qy), ptr(qz), itp_strategy.code, st.ctypes.data),
+            "traversal_stats")
+    return st
+
+
 def LBVH_query(lbvh, points, radius):
     """Batched LBVH_query!: one NeighborSelection per point (radius scalar or per point)."""
     qx, qy, qz = _pts(points)

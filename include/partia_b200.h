@@ -109,6 +109,15 @@ int32_t pb_query_count(pb_handle *h, int64_t npts, const double *qx, const doubl
 int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
                            const double *radius, const int64_t *offsets, int64_t *pool, int64_t *nearest);
 
+/* Event counts of the reference traversal algorithm on the last build (leaf size 1, Karras
+   tree, left-first DFS, FP64 boxes; LinearBVHTraversalMacros.jl:26-371 driven as in
+   PointSamples_interpolation.jl:118-133).  stats is [npts][5]: nearest-pass internal visits,
+   nearest-pass leaf tests, main-pass internal visits, main-pass leaf tests, accepted
+   neighbours.  These define the algorithmic-bytes model of the traversal and are the exact
+   per-query work labels of the learned schedule. */
+int32_t pb_traversal_stats(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                           int32_t strategy, int64_t *stats);
+
 /* Per-point kernel loop of PointSamples_interpolation on the last build
    (Partia.jl/src/julia/KernelInterpolation/grid_interpolation/PointSamples_interpolation.jl:99-184):
    LBVH_find_nearest_h + _general_quantity_interpolate_kernel (general_interpolation.jl:1-669).

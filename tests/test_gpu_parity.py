@@ -275,3 +275,16 @@ def test_device_resident_inputs(backend):
     _assert_same(got, exp)
     _, order = lb.encoding()
     assert np.array_equal(dev["x"].cpu().numpy(), p["x"][order])
+
+
+@pytest.mark.parametrize("strategy", ["itpGather", "itpScatter", "itpSymmetric"])
+def test_traversal_stats_match_oracle(backend, strategy):
+    p = synthetic.disc(20000, seed=17)
+    inp = _input(p)
+    lb = pb.LinearBVH_build(inp, backend)
+    grid = synthetic.cartesian_box_grid(p, n=12, pad=1.0)
+    flat = pb.flatten(pb.Cartesian, grid)
+    st = pb.traversal_stats(lb, flat.coor, getattr(pb, strategy))
+    cat = pb.InterpolationCatalog(COLS, scalars=("rho",))
+    _, exp = _oracle(p).interp_points(cat.oracle_dict(), *flat.coor, strategy=strategy, stats=True)
+    assert np.array_equal(st, exp)
