@@ -28,6 +28,7 @@ UNITS = {
     "pb_query.cu": ["-fmad=false"],
     "pb_interp32.cu": ["-fmad=true"],
     "pb_capi.cu": [],
+    "pb_noalloc.cu": ["-fmad=false"],
 }
 HEADERS = ["pb_device.cuh", "pb_internal.h", "pb_interp_impl.cuh", "line_tables.h"]
 

@@ -60,7 +60,7 @@ class PBCatalog(ctypes.Structure):
 EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set_option", "pb_linear_bvh",
             "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors", "pb_traversal_stats",
             "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
-            "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings"]
+            "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc"]
 
 _lib = None
 
@@ -99,6 +99,7 @@ def load():
                                           [_vp] * 6 + [ctypes.c_int32, ctypes.c_int32, P(_vp), ctypes.c_int32]),
         "pb_launch_count": (ctypes.c_int64, [_vp]),
         "pb_last_timings": (ctypes.c_int32, [_vp, _dp, _dp, _lp]),
+        "pb_morton_sort_noalloc": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

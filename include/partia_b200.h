@@ -148,6 +148,20 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
                                       const double *dy, const double *dz, int32_t strategy, int32_t precision,
                                       double *const *out, int32_t flags);
 
+/* Morton encode + stable radix sort + duplicate bump of the LBVH build (the sorted
+   MortonEncoding codes and the 0-based sorting order) without allocating any device memory.
+   This entry point has no counterpart in the reference: it exists for callers that cannot
+   call cudaMalloc -- applications that own all device memory through their own pool, or
+   pipelines that cannot take the synchronisation an allocation may imply.  Its sort scratch
+   is one fixed static device array (about 6.3 MB per GPU, held until exit) shared by every
+   call: n <= PB_NOALLOC_MAX_N (larger n returns PB_ERR_CAPACITY), calls whose GPU work
+   overlaps race on it, and the first call on a device (which looks up the array's address)
+   should come before any stream capture.  x, y, z, codes_out, order_out are device pointers;
+   the call is synchronous on `cuda_stream` (NULL = the default stream). */
+#define PB_NOALLOC_MAX_N 262144
+int32_t pb_morton_sort_noalloc(const double *x, const double *y, const double *z, int64_t n, uint64_t *codes_out,
+                               int64_t *order_out, void *cuda_stream);
+
 /* Diagnostics: kernels launched by this handle so far; build / traversal device time of
    the last call in ms (needs option "timing"); traversal kernel launches of the last call. */
 int64_t pb_launch_count(const pb_handle *h);
