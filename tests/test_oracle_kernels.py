@@ -1,0 +1,147 @@
+"""Known-answer tests of the oracle's SPH kernel functions and line-integrated tables.
+
+Restates Partia.jl/test/kernel_function_tests.jl (support radii, normalisation constants,
+analytic values at q in {0, .3, .7, 1, 1.3, 1.8} with atol 1e-14, compact support, NaN for
+q < 0, gradient vs finite difference, W(r, h) scaling, line-integrated two-point form) and
+checks the regenerated line-integrated tables against the reference's tabulated values.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+KERNELS = ["M4_spline", "M5_spline", "M6_spline", "C2_Wendland", "C4_Wendland", "C6_Wendland"]
+
+
+def analytic(k, q):
+    if q < 0:
+        return math.nan
+    if k == "M4_spline":
+        return 0.0 if q >= 2 else (0.25 * (2 - q) ** 3 - (1 - q) ** 3 if q < 1 else 0.25 * (2 - q) ** 3)
+    if k == "M5_spline":
+        if q >= 2.5:
+            return 0.0
+        if q < 0.5:
+            return (2.5 - q) ** 4 - 5 * (1.5 - q) ** 4 + 10 * (0.5 - q) ** 4
+        return (2.5 - q) ** 4 - 5 * (1.5 - q) ** 4 if q < 1.5 else (2.5 - q) ** 4
+    if k == "M6_spline":
+        if q >= 3:
+            return 0.0
+        if q < 1:
+            return (3 - q) ** 5 - 6 * (2 - q) ** 5 + 15 * (1 - q) ** 5
+        return (3 - q) ** 5 - 6 * (2 - q) ** 5 if q < 2 else (3 - q) ** 5
+    if q >= 2:
+        return 0.0
+    t = 1 - 0.5 * q
+    if k == "C2_Wendland":
+        return t ** 4 * (2 * q + 1)
+    if k == "C4_Wendland":
+        return t ** 6 * (35 / 12 * q ** 2 + 3 * q + 1)
+    return t ** 8 * (4 * q ** 3 + 6.25 * q ** 2 + 4 * q + 1)
+
+
+def test_support_radii():
+    exp = {"M4_spline": 2.0, "M5_spline": 2.5, "M6_spline": 3.0, "C2_Wendland": 2.0, "C4_Wendland": 2.0,
+           "C6_Wendland": 2.0}
+    for k, v in exp.items():
+        assert oracle.kernel_valid(k) == v
+
+
+def test_normalisation_constants():
+    exp = {"M4_spline": 1 / math.pi, "C2_Wendland": 21 / (16 * math.pi), "C4_Wendland": 495 / (256 * math.pi),
+           "M5_spline": 0.05 / math.pi, "M6_spline": 1 / (120 * math.pi), "C6_Wendland": 1365 / (512 * math.pi)}
+    for k, v in exp.items():
+        assert oracle.kernel_norm3(k) == pytest.approx(v, rel=1e-15)
+
+
+@pytest.mark.parametrize("k", KERNELS)
+def test_kernel_values(k):
+    s = oracle.kernel_norm3(k)
+    for q in (0.0, 0.3, 0.7, 1.0, 1.3, 1.8):
+        assert abs(s * oracle.kernel_f(k, q) - s * analytic(k, q)) <= 1e-14
+
+
+@pytest.mark.parametrize("k", KERNELS)
+def test_compact_support_and_negative_q(k):
+    qmax = oracle.kernel_valid(k)
+    assert oracle.kernel_f(k, qmax + 0.1) == 0.0
+    assert oracle.kernel_f(k, qmax + 10.0) == 0.0
+    assert math.isnan(oracle.kernel_f(k, -0.1))
+
+
+@pytest.mark.parametrize("k", KERNELS)
+def test_gradient_finite_difference(k):
+    h, ra, rb, d = 0.1, (0.5, 0.5, 0.5), (0.55, 0.52, 0.48), 1e-6
+    r0 = math.dist(ra, rb)
+    r1 = math.dist(ra, (rb[0] + d, rb[1], rb[2]))
+    fd = (oracle.W(k, r1, h) - oracle.W(k, r0, h)) / d
+    g = oracle.gradW(k, rb[0] - ra[0], rb[1] - ra[1], rb[2] - ra[2], h)
+    assert g[0] == pytest.approx(fd, rel=1e-4)
+
+
+def test_W_scaling():
+    h, r = 0.15, 0.2
+    exp = oracle.kernel_norm3("M4_spline") * analytic("M4_spline", r / h) / h ** 3
+    assert abs(oracle.W("M4_spline", r, h) - exp) <= 1e-14
+
+
+def test_line_kernel_two_point_interface():
+    h, ra, rb = 0.1, (0.5, 0.5), (0.52, 0.48)
+    r = math.sqrt((ra[0] - rb[0]) ** 2 + (ra[1] - rb[1]) ** 2)
+    dx, dy = ra[0] - rb[0], ra[1] - rb[1]
+    r2 = math.sqrt(dx * dx + dy * dy)
+    assert abs(oracle.line_W("M4_spline", r, h) - oracle.line_W("M4_spline", r2, h)) <= 1e-14
+
+
+def test_line_kernel_integrates_3d_kernel():
+    # The reference scales the normalised column table by 1/h (line_integrated_kernel.jl:132-137),
+    # while the column integral of W itself is table / h^2, so the reference's line kernel equals
+    # h * integral W ds; the restatement keeps that scaling.
+    h, r = 0.3, 0.17
+    s = np.linspace(-2 * h, 2 * h, 200001)
+    w = np.array([oracle.W("M4_spline", math.hypot(r, si), h) for si in s[::50]])
+    num = np.trapezoid(w, s[::50])
+    assert oracle.line_W("M4_spline", r, h) == pytest.approx(num * h, rel=2e-3)
+
+
+def test_jl_pow_matches_exact_power():
+    from fractions import Fraction
+    rng = np.random.default_rng(0)
+    for x in rng.uniform(0.0, 1.0, 200):
+        for n in (4, 5, 6, 7, 8):
+            exact = float(Fraction(float(x)) ** n)
+            got = oracle.jl_pow(x, n)
+            assert abs(got - exact) <= np.spacing(exact)
+
+
+def test_line_tables_match_reference_samples():
+    from golden import load
+    ref = load("line_table_samples")
+    here = os.path.dirname(os.path.abspath(__file__))
+    import sys
+    sys.path.insert(0, os.path.join(here, "..", "distorteddustydiscanalysistoolkits_b200", "csrc"))
+    import gen_line_tables as g
+    tabs = g.tables()
+    for name, d in ref.items():
+        ours = tabs[name][1][np.array(d["index"])]
+        assert np.max(np.abs(ours - np.array(d["value"]))) <= 1e-9, name
+
+
+def test_line_tables_match_full_reference_file():
+    path = "/root/reference/Partia.jl/src/julia/KernelInterpolation/table/line_integrated_kernel_tables.jl"
+    if not os.path.exists(path):
+        pytest.skip("reference checkout not present")
+    import re
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "..", "distorteddustydiscanalysistoolkits_b200", "csrc"))
+    import gen_line_tables as g
+    tabs = g.tables()
+    txt = open(path).read()
+    for name, body in re.findall(r"const _(\w+)_Inorm = SVector\{4096,Float64\}\(([^)]*)\)", txt, re.S):
+        v = np.array([float(s) for s in body.replace("\n", "").split(",") if s.strip()])
+        assert np.max(np.abs(tabs[name][1] - v)) <= 1e-9, name
