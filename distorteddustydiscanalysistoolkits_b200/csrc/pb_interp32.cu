@@ -9,8 +9,9 @@
 //     pair needs no division and no FP64 column arithmetic;
 //   * kernel shapes are evaluated branch-free from their truncated-power forms
 //     (M4: 0.25 (2-q)_+^3 - (1-q)_+^3, ...), templated on the kernel type;
-//   * every quantity enters as an offset A_b - A_hat (A_hat = first accepted neighbour's
-//     value, as a double-float) so that gradient/divergence/curl F - A B does not cancel;
+//   * every quantity enters as an offset A_b - A_hat (A_hat = the nearest particle's value,
+//     or the first accepted neighbour's for scatter, as a double-float) so that
+//     gradient/divergence/curl F - A B cancels as little as possible;
 //   * sums are accumulated per chunk of 4 accepted pairs in plain FP32 and each chunk sum
 //     is folded into a TwoSum-compensated accumulator.
 // The per-query arithmetic depends only on the query and the tree (chunks are counted over
@@ -25,39 +26,54 @@ __device__ const float g_line_inorm32[6][PB_LINE_NTAB] = PB_LINE_INORM_INIT;
 
 constexpr int CHUNK = 4;
 
-// ---- branch-free kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) ----
+// ---- kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) in FP32 ----
+// Algebraically identical to the reference's piecewise forms but arranged so that nothing
+// cancels near q = 0 (where f'(q) -> 0): the innermost piece of every spline and every
+// Wendland derivative is expanded into a polynomial with an explicit factor q, e.g. M4
+// f'(q) = -0.75 (2-q)^2 + 3 (1-q)^2 = q (2.25 q - 3) for q < 1, and C4
+// f'(q) = t^5 (t (35/6 q + 3) - (35/4 q^2 + 9 q + 3)) = -(14/3) q (1 + 2.5 q) t^5, t = 1 - q/2.
+// Pieces are chosen with selects, so lanes never diverge.
 template <int KT>
 __device__ __forceinline__ void shape(float q, float &f, float &df)
 {
     if (KT == 0) {   // M4
-        float a = fmaxf(2.f - q, 0.f), b = fmaxf(1.f - q, 0.f);
-        f = 0.25f * a * a * a - b * b * b;
-        df = -0.75f * a * a + 3.f * b * b;
+        float a = fmaxf(2.f - q, 0.f);
+        float fi = 1.f + q * q * (0.75f * q - 1.5f), di = q * (2.25f * q - 3.f);
+        float fo = 0.25f * a * a * a, dO = -0.75f * a * a;
+        bool in = q < 1.f;
+        f = in ? fi : fo;
+        df = in ? di : dO;
     } else if (KT == 1) {   // M5
         float a = fmaxf(2.5f - q, 0.f), b = fmaxf(1.5f - q, 0.f), c = fmaxf(0.5f - q, 0.f);
         float a2 = a * a, b2 = b * b, c2 = c * c;
         f = a2 * a2 - 5.f * b2 * b2 + 10.f * c2 * c2;
-        df = -4.f * a2 * a + 20.f * b2 * b - 40.f * c2 * c;
+        float q2 = q * q;
+        float di = q * (24.f * q2 - 30.f);
+        float dO = -4.f * a2 * a + 20.f * b2 * b;
+        df = q < 0.5f ? di : dO;
     } else if (KT == 2) {   // M6
         float a = fmaxf(3.f - q, 0.f), b = fmaxf(2.f - q, 0.f), c = fmaxf(1.f - q, 0.f);
         float a4 = (a * a) * (a * a), b4 = (b * b) * (b * b), c4 = (c * c) * (c * c);
         f = a4 * a - 6.f * b4 * b + 15.f * c4 * c;
-        df = -5.f * a4 + 30.f * b4 - 75.f * c4;
+        float q2 = q * q;
+        float di = q * (q2 * (120.f - 50.f * q) - 120.f);
+        float dO = -5.f * a4 + 30.f * b4;
+        df = q < 1.f ? di : dO;
     } else if (KT == 3) {   // C2
         float t = fmaxf(1.f - 0.5f * q, 0.f);
         float t3 = t * t * t;
         f = t3 * t * (2.f * q + 1.f);
-        df = t3 * (2.f * t - (4.f * q + 2.f));
+        df = -5.f * q * t3;
     } else if (KT == 4) {   // C4
         float t = fmaxf(1.f - 0.5f * q, 0.f);
         float t5 = (t * t) * (t * t) * t;
         f = t5 * t * ((35.f / 12.f) * q * q + 3.f * q + 1.f);
-        df = t5 * (t * ((35.f / 6.f) * q + 3.f) - ((35.f / 4.f) * q * q + 9.f * q + 3.f));
+        df = -(14.f / 3.f) * q * (1.f + 2.5f * q) * t5;
     } else {   // C6
         float t = fmaxf(1.f - 0.5f * q, 0.f);
         float t7 = (t * t) * (t * t) * (t * t) * t;
         f = t7 * t * (((4.f * q + 6.25f) * q + 4.f) * q + 1.f);
-        df = t7 * (t * ((12.f * q + 12.5f) * q + 4.f) - (((16.f * q + 25.f) * q + 16.f) * q + 4.f));
+        df = -5.5f * q * ((4.f * q + 3.5f) * q + 1.f) * t7;
     }
 }
 
@@ -305,9 +321,10 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
         double ha = 0.0;
         Query32 Q{0.f, 0.f, 0.f};
+        int64_t bnear = -1;
         if (STRAT != SCATTER) {
-            int64_t b = nearest_leaf(T, px, py, pz);
-            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
+            bnear = nearest_leaf(T, px, py, pz);
+            ha = bnear < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + bnear).w;
             float ih = (float)(1.0 / ha);
             Q.ih = ih;
             Q.cw = sig * ih * ih * ih;
@@ -316,6 +333,20 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
         Acc32 A;
         A.init();
+        if (bnear >= 0) {
+            // quantities enter as offsets from the nearest particle's values, which are close
+            // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
+            const float4 *rec = pay + bnear * stride;
+#pragma unroll
+            for (int k = 1; k <= (MAXU + 1) / 2; ++k) {
+                if (k < stride) {
+                    float4 c = __ldg(rec + k);
+                    A.hh[2 * k - 2] = c.x; A.hl[2 * k - 2] = c.y;
+                    if (2 * k - 1 < MAXU) { A.hh[2 * k - 1] = c.z; A.hl[2 * k - 1] = c.w; }
+                }
+            }
+            A.have = true;
+        }
         Slots S{0, -1};
         auto proc = [&](int fill) {
             if (!A.have) {
