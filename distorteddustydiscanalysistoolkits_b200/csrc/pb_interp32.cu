@@ -90,27 +90,37 @@ __device__ __forceinline__ float ldexp_norm3(int k)
     }
 }
 
-// payload: record of stride float4s per sorted particle
-//   [0] = {1/h, sigma h^-3, sigma h^-4, m/rho}, then (hi, lo) pairs of the launch's columns
+// payload: record of `stride` float4s per sorted particle
+//   [0] = {x_hi, y_hi, z_hi, 1/h}, [1] = {x_lo, y_lo, z_lo, m/rho}, [2] = {sigma h^-3, sigma h^-4, A0_hi, A0_lo},
+//   [3..] = remaining (hi, lo) column pairs.  Coordinates are double-float pairs, so the pair
+//   offset x_a - x_b is formed in FP32 as (xa_hi - xb_hi) + (xa_lo - xb_lo) without FP64 loads.
+__host__ __device__ inline int payload_stride(int nU) { return 2 + (2 + 2 * nU + 3) / 4; }
+
 __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int stride)
 {
     const float sig = ldexp_norm3(T.kernel);
     for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x) {
-        double h = T.leaf[b].w;
-        double ih = 1.0 / h;
-        float4 p0 = make_float4((float)ih, (float)(sig * ih * ih * ih), (float)(sig * ih * ih * ih * ih),
-                                (float)(T.m[b] / T.rho[b]));
+        double4 L = T.leaf[b];
+        double ih = 1.0 / L.w;
+        float xh = (float)L.x, yh = (float)L.y, zh = (float)L.z;
         float4 *rec = pay + b * stride;
-        rec[0] = p0;
-        float v[2 * MAXU];
+        rec[0] = make_float4(xh, yh, zh, (float)ih);
+        rec[1] = make_float4((float)(L.x - (double)xh), (float)(L.y - (double)yh), (float)(L.z - (double)zh),
+                             (float)(T.m[b] / T.rho[b]));
+        float v[2 + 2 * MAXU + 2];
+        v[0] = (float)(sig * ih * ih * ih);
+        v[1] = (float)(sig * ih * ih * ih * ih);
 #pragma unroll
         for (int u = 0; u < MAXU; ++u) {
             double a = (u < C.nU) ? C.ucol[u][b] : 0.0;
             float hi = (float)a;
-            v[2 * u] = hi;
-            v[2 * u + 1] = (float)(a - (double)hi);
+            v[2 + 2 * u] = hi;
+            v[3 + 2 * u] = (float)(a - (double)hi);
         }
-        for (int k = 1; k < stride; ++k) rec[k] = make_float4(v[4 * k - 4], v[4 * k - 3], v[4 * k - 2], v[4 * k - 1]);
+        v[2 + 2 * MAXU] = 0.f;
+        v[3 + 2 * MAXU] = 0.f;
+        for (int k = 2; k < stride; ++k)
+            rec[k] = make_float4(v[4 * k - 8], v[4 * k - 7], v[4 * k - 6], v[4 * k - 5]);
     }
 }
 
@@ -180,15 +190,35 @@ struct Acc32 {
 
 struct Query32 {
     float ih, cw, cg;   // 1/h_a, sigma h_a^-3, sigma h_a^-4
+    float ph[3], pl[3]; // query position as double-float pairs
 };
+
+// kernel constants and column value pairs (hi, lo) of a record
+__device__ __forceinline__ void load_cols(const float4 *rec, int stride, float &cW, float &cG, float *ch, float *cl)
+{
+    float v[4 * 4];
+#pragma unroll
+    for (int k = 2; k < 6; ++k) {
+        float4 c = (k < stride) ? __ldg(rec + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[4 * k - 8] = c.x; v[4 * k - 7] = c.y; v[4 * k - 6] = c.z; v[4 * k - 5] = c.w;
+    }
+    cW = v[0];
+    cG = v[1];
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) { ch[u] = v[2 + 2 * u]; cl[u] = v[3 + 2 * u]; }
+}
 
 template <int STRAT, int KT>
 __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
-                                       const float4 *__restrict__ pay, int stride, int64_t b, float dx, float dy,
-                                       float dz)
+                                       const float4 *__restrict__ pay, int stride, int64_t b)
 {
     const float4 *rec = pay + b * stride;
-    float4 p0 = __ldg(rec);
+    float4 p0 = __ldg(rec), p1 = __ldg(rec + 1);
+    float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
+    float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
+    float dz = (Q.ph[2] - p0.z) + (Q.pl[2] - p1.z);
+    float cWb, cGb, ch[MAXU], cl[MAXU];
+    load_cols(rec, stride, cWb, cGb, ch, cl);
     float r2 = dx * dx + dy * dy + dz * dz;
     float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
     float r = r2 * rinv;
@@ -196,9 +226,9 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_
     if (STRAT == SYMMETRIC) {
         float fa, dfa, fb, dfb;
         shape<KT>(r * Q.ih, fa, dfa);
-        shape<KT>(r * p0.x, fb, dfb);
-        W = 0.5f * (Q.cw * fa + p0.y * fb);
-        G = 0.5f * (Q.cg * dfa + p0.z * dfb) * rinv;
+        shape<KT>(r * p0.w, fb, dfb);
+        W = 0.5f * (Q.cw * fa + cWb * fb);
+        G = 0.5f * (Q.cg * dfa + cGb * dfb) * rinv;
     } else if (STRAT == GATHER) {
         float f, df;
         shape<KT>(r * Q.ih, f, df);
@@ -206,28 +236,20 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_
         G = Q.cg * df * rinv;
     } else {
         float f, df;
-        shape<KT>(r * p0.x, f, df);
-        W = p0.y * f;
-        G = p0.z * df * rinv;
+        shape<KT>(r * p0.w, f, df);
+        W = cWb * f;
+        G = cGb * df * rinv;
     }
-    float w = p0.w * W;
+    const float mrho = p1.w;
+    float w = mrho * W;
     float a[MAXU];
 #pragma unroll
-    for (int k = 1; k <= (MAXU + 1) / 2; ++k) {
-        if (k < stride) {
-            float4 c = __ldg(rec + k);
-            a[2 * k - 2] = (c.x - A.hh[2 * k - 2]) + (c.y - A.hl[2 * k - 2]);
-            if (2 * k - 1 < MAXU) a[2 * k - 1] = (c.z - A.hh[2 * k - 1]) + (c.w - A.hl[2 * k - 1]);
-        } else {
-            a[2 * k - 2] = 0.f;
-            if (2 * k - 1 < MAXU) a[2 * k - 1] = 0.f;
-        }
-    }
+    for (int u = 0; u < MAXU; ++u) a[u] = (ch[u] - A.hh[u]) + (cl[u] - A.hl[u]);
     A.pS1 += w;
 #pragma unroll
     for (int u = 0; u < MAXU; ++u) A.pSA[u] += a[u] * w;
     if (need_grad) {
-        float gq = p0.w * G;
+        float gq = mrho * G;
         float gx = gq * dx, gy = gq * dy, gz = gq * dz;
         A.pB[0] += gx; A.pB[1] += gy; A.pB[2] += gz;
 #pragma unroll
@@ -320,7 +342,7 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         if (qi >= nq) continue;
         double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
         double ha = 0.0;
-        Query32 Q{0.f, 0.f, 0.f};
+        Query32 Q{};
         int64_t bnear = -1;
         if (STRAT != SCATTER) {
             bnear = nearest_leaf(T, px, py, pz);
@@ -331,42 +353,26 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
             Q.cg = Q.cw * ih;
         }
         double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
+        Q.ph[0] = (float)px; Q.pl[0] = (float)(px - (double)Q.ph[0]);
+        Q.ph[1] = (float)py; Q.pl[1] = (float)(py - (double)Q.ph[1]);
+        Q.ph[2] = (float)pz; Q.pl[2] = (float)(pz - (double)Q.ph[2]);
         Acc32 A;
         A.init();
+        float cw_, cg_;
         if (bnear >= 0) {
             // quantities enter as offsets from the nearest particle's values, which are close
             // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
-            const float4 *rec = pay + bnear * stride;
-#pragma unroll
-            for (int k = 1; k <= (MAXU + 1) / 2; ++k) {
-                if (k < stride) {
-                    float4 c = __ldg(rec + k);
-                    A.hh[2 * k - 2] = c.x; A.hl[2 * k - 2] = c.y;
-                    if (2 * k - 1 < MAXU) { A.hh[2 * k - 1] = c.z; A.hl[2 * k - 1] = c.w; }
-                }
-            }
+            load_cols(pay + bnear * stride, stride, cw_, cg_, A.hh, A.hl);
             A.have = true;
         }
         Slots S{0, -1};
         auto proc = [&](int fill) {
             if (!A.have) {
                 int64_t b0 = __shfl_sync(0xffffffffu, S.mine, 0);
-                const float4 *rec = pay + b0 * stride;
-#pragma unroll
-                for (int k = 1; k <= (MAXU + 1) / 2; ++k) {
-                    if (k < stride) {
-                        float4 c = __ldg(rec + k);
-                        A.hh[2 * k - 2] = c.x; A.hl[2 * k - 2] = c.y;
-                        if (2 * k - 1 < MAXU) { A.hh[2 * k - 1] = c.z; A.hl[2 * k - 1] = c.w; }
-                    }
-                }
+                load_cols(pay + b0 * stride, stride, cw_, cg_, A.hh, A.hl);
                 A.have = true;
             }
-            if (S.mine >= 0) {
-                double4 L = ldg4(T.leaf + S.mine);
-                pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, S.mine, (float)(px - L.x), (float)(py - L.y),
-                                  (float)(pz - L.z));
-            }
+            if (S.mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, S.mine);
         };
         if (T.root == 0) {
             double4 L;
@@ -434,7 +440,7 @@ static void launch_kt(Handle *H, const DevTree &T, const DevCatalog &C, const fl
 cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
                                const double *qx, const double *qy, const double *qz, const uint32_t *perm)
 {
-    int stride = 1 + (C.nU + 1) / 2;
+    int stride = payload_stride(C.nU);
     cudaError_t e = H->payload.reserve(sizeof(float4) * stride * T.n);
     if (e) return e;
     e = H->counter.reserve(sizeof(unsigned long long));

@@ -41,6 +41,52 @@ __device__ __forceinline__ NodeF load_node(const NodeF *p)
     return nd;
 }
 
+// --------------------------------------------------------------------------------------
+// FP32 box tests with directed rounding.  The query point is kept as round-down/round-up
+// floats; gaps, squares and sums are rounded toward the safe side, so `lower` never exceeds
+// the exact box distance^2 and `upper` is never below the exact farthest-corner distance^2.
+// Decisions then carry a relative margin of 2^-20, far above FP64 rounding (2^-53), so a
+// subtree is pruned only if every leaf in it fails its FP64 acceptance test and is
+// bulk-accepted only if every leaf passes it -- exactly the decisions of the FP64 walk.
+struct QBox {
+    float dn[3], up[3];
+};
+
+__device__ __forceinline__ QBox make_qbox(double px, double py, double pz)
+{
+    QBox q;
+    q.dn[0] = __double2float_rd(px); q.up[0] = __double2float_ru(px);
+    q.dn[1] = __double2float_rd(py); q.up[1] = __double2float_ru(py);
+    q.dn[2] = __double2float_rd(pz); q.up[2] = __double2float_ru(pz);
+    return q;
+}
+
+constexpr float MARGIN_UP = 1.0f + 9.5367431640625e-07f;   // 1 + 2^-20
+constexpr float MARGIN_DN = 1.0f - 9.5367431640625e-07f;
+
+__device__ __forceinline__ float box_lower(const QBox &q, const NodeF &nd)
+{
+    float gx = fmaxf(fmaxf(__fsub_rd(nd.lox, q.up[0]), __fsub_rd(q.dn[0], nd.hix)), 0.f);
+    float gy = fmaxf(fmaxf(__fsub_rd(nd.loy, q.up[1]), __fsub_rd(q.dn[1], nd.hiy)), 0.f);
+    float gz = fmaxf(fmaxf(__fsub_rd(nd.loz, q.up[2]), __fsub_rd(q.dn[2], nd.hiz)), 0.f);
+    return __fadd_rd(__fadd_rd(__fmul_rd(gx, gx), __fmul_rd(gy, gy)), __fmul_rd(gz, gz));
+}
+
+__device__ __forceinline__ float box_upper(const QBox &q, const NodeF &nd)
+{
+    float fx = fmaxf(__fsub_ru(q.up[0], nd.lox), __fsub_ru(nd.hix, q.dn[0]));
+    float fy = fmaxf(__fsub_ru(q.up[1], nd.loy), __fsub_ru(nd.hiy, q.dn[1]));
+    float fz = fmaxf(__fsub_ru(q.up[2], nd.loz), __fsub_ru(nd.hiz, q.dn[2]));
+    return __fadd_ru(__fadd_ru(__fmul_ru(fx, fx), __fmul_ru(fy, fy)), __fmul_ru(fz, fz));
+}
+
+// (K h)^2 rounded up, for a node's hmax (already rounded up) or the query radius
+__device__ __forceinline__ float sq_up(float K, float h)
+{
+    float r = __fmul_ru(K, h);
+    return __fmul_ru(r, r);
+}
+
 // LBVH_find_nearest_h (LinearBVHQueries.jl:118-140).  The reference walks the tree in DFS
 // order with a shrinking radius and keeps the first strictly closer leaf, i.e. it returns
 // the minimum squared distance and, among equal distances, the smallest sorted leaf index.
@@ -50,8 +96,8 @@ __device__ __forceinline__ NodeF load_node(const NodeF *p)
 // when its box distance is strictly greater than the best distance.
 constexpr int NN_STACK = 64;
 
-__device__ __forceinline__ double child_dist(const DevTree &T, int id, double px, double py, double pz,
-                                             double &best, int64_t &bi)
+__device__ __forceinline__ float child_dist(const DevTree &T, const QBox &q, int id, double px, double py,
+                                            double pz, double &best, int64_t &bi)
 {
     const int64_t n = T.n;
     if (id >= n) {
@@ -60,7 +106,7 @@ __device__ __forceinline__ double child_dist(const DevTree &T, int id, double px
         if (d2 < best || (d2 == best && b < bi)) { best = d2; bi = b; }
         return INFINITY;   // a leaf needs no further visit
     }
-    return d2_box(px, py, pz, load_node(T.node + (id - 1)));
+    return box_lower(q, load_node(T.node + (id - 1)));
 }
 
 __device__ __forceinline__ int64_t nearest_leaf(const DevTree &T, double px, double py, double pz)
@@ -71,21 +117,24 @@ __device__ __forceinline__ int64_t nearest_leaf(const DevTree &T, double px, dou
         double d2 = d2_point(px, py, pz, ldg4(T.leaf));
         return d2 < best ? 0 : -1;
     }
+    const QBox q = make_qbox(px, py, pz);
     int sn[NN_STACK];
-    double sd[NN_STACK];
+    float sd[NN_STACK];
     int sp = 0;
     int node = T.root;
     int64_t guard = 0, limit = 4 * T.n + 64;
+    // a subtree is skipped only when its lower bound exceeds the best distance by the margin
+    auto visit = [&](float d) { return d <= __fmul_ru(__double2float_ru(best), MARGIN_UP); };
     for (;;) {
         if (++guard > limit) { atomicOr(T.status, ST_TRAVERSAL); break; }
         int2 ch = __ldg(T.child + (node - 1));
-        double dl = child_dist(T, ch.x, px, py, pz, best, bi);
-        double dr = child_dist(T, ch.y, px, py, pz, best, bi);
-        bool vl = dl <= best, vr = dr <= best;
+        float dl = child_dist(T, q, ch.x, px, py, pz, best, bi);
+        float dr = child_dist(T, q, ch.y, px, py, pz, best, bi);
+        bool vl = visit(dl), vr = visit(dr);
         if (vl && vr) {
             bool lf = dl <= dr;
             int far = lf ? ch.y : ch.x;
-            double fd = lf ? dr : dl;
+            float fd = lf ? dr : dl;
             if (sp < NN_STACK) { sn[sp] = far; sd[sp] = fd; ++sp; }
             else { atomicOr(T.status, ST_TRAVERSAL); }
             node = lf ? ch.x : ch.y;
@@ -96,7 +145,7 @@ __device__ __forceinline__ int64_t nearest_leaf(const DevTree &T, double px, dou
         node = 0;
         while (sp > 0) {
             --sp;
-            if (sd[sp] <= best) { node = sn[sp]; break; }
+            if (visit(sd[sp])) { node = sn[sp]; break; }
         }
         if (node == 0) break;
     }
@@ -187,6 +236,10 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
                                           double r2a, int64_t &lo, int64_t &hi)
 {
     const int64_t n = T.n;
+    const QBox q = make_qbox(px, py, pz);
+    const float Kf = (float)K;
+    const float r2a_up = __double2float_ru(r2a);
+    const float bulk_lim = __fmul_rd(__double2float_rd(r2a), MARGIN_DN);
     for (;;) {
         if (w.node == 0) return false;
         if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.node = 0; return false; }
@@ -206,15 +259,14 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
             continue;
         }
         NodeF nd = load_node(T.node + (node - 1));
-        double r2;
-        if (STRAT == GATHER) r2 = r2a;
+        float r2n;
+        if (STRAT == GATHER) r2n = r2a_up;
         else {
-            double r = __dmul_rn(K, (double)__ldg(T.node_hmax + (node - 1)));
-            double rr = __dmul_rn(r, r);
-            r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+            float rr = sq_up(Kf, __ldg(T.node_hmax + (node - 1)));
+            r2n = STRAT == SCATTER ? rr : fmaxf(r2a_up, rr);
         }
-        if (d2_box(px, py, pz, nd) > r2) { w.node = nd.escape; continue; }
-        if (STRAT != SCATTER && far_d2_box(px, py, pz, nd) <= r2a) {
+        if (box_lower(q, nd) > __fmul_ru(r2n, MARGIN_UP)) { w.node = nd.escape; continue; }
+        if (STRAT != SCATTER && box_upper(q, nd) <= bulk_lim) {
             int2 rg = __ldg(T.range + (node - 1));
             lo = rg.x;
             hi = rg.y;
