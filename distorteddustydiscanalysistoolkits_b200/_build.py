@@ -26,6 +26,7 @@ UNITS = {
     "pb_build.cu": ["-fmad=false"],
     "pb_interp64.cu": ["-fmad=false"],
     "pb_query.cu": ["-fmad=false"],
+    "pb_walk.cu": ["-fmad=false"],
     "pb_interp32.cu": ["-fmad=true"],
     "pb_capi.cu": [],
     "pb_noalloc.cu": ["-fmad=false"],

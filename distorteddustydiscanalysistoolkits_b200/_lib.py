@@ -60,7 +60,8 @@ class PBCatalog(ctypes.Structure):
 EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set_option", "pb_linear_bvh",
             "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors", "pb_traversal_stats",
             "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
-            "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc"]
+            "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc",
+            "pb_last_schedule"]
 
 _lib = None
 
@@ -99,6 +100,7 @@ def load():
                                           [_vp] * 6 + [ctypes.c_int32, ctypes.c_int32, P(_vp), ctypes.c_int32]),
         "pb_launch_count": (ctypes.c_int64, [_vp]),
         "pb_last_timings": (ctypes.c_int32, [_vp, _dp, _dp, _lp]),
+        "pb_last_schedule": (ctypes.c_int32, [_vp, _lp, _lp, _lp]),
         "pb_morton_sort_noalloc": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
@@ -179,3 +181,9 @@ class Handle:
         b, i, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
         self.lib.pb_last_timings(self.h, ctypes.byref(b), ctypes.byref(i), ctypes.byref(n))
         return b.value, i.value, n.value
+
+    def schedule(self):
+        """(walk rounds, deferred queries, pool chunks) of the last FP32-compensated point call."""
+        r, d, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self.lib.pb_last_schedule(self.h, ctypes.byref(r), ctypes.byref(d), ctypes.byref(c))
+        return r.value, d.value, c.value

@@ -6,6 +6,7 @@
 // checks, and optional CUDA-event timing of the build and traversal stages.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -24,7 +25,9 @@ pb::Handle::~Handle()
     DBuf *all[] = {&in_x, &in_y, &in_z, &in_h, &in_m, &in_rho, &codes, &codes_alt, &idx, &idx_alt, &scan_tmp,
                    &scan_part, &hist, &bbox_part, &qparams, &status, &leaf, &leaf_escape, &node, &node_hmax, &node_child, &node_range, &payload, &counter, &left,
                    &right, &escape, &parent, &bmin64, &bmax64, &hmax64, &counters, &m_s, &rho_s, &col_ptrs,
-                   &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux};
+                   &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux,
+                   &pool_runs, &pool_next, &pool_ctr, &items, &wbnear, &qacc, &qflag, &cut, &defer_a, &defer_b,
+                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota};
     for (DBuf *b : all) b->release();
     for (auto &b : in_cols) b.release();
     for (auto &b : cols_s) b.release();
@@ -402,6 +405,132 @@ int do_build(Handle &H, const pb_input *in, int32_t flags)
     return PB_OK;
 }
 
+// Run pool of the two-phase point path.  Its size follows the number of queries (24 chunks
+// of 32 runs per query), bounded by a sixth of the device memory (at most 24 GiB), by
+// PB_RUN_POOL_MB, or set exactly in chunks by PB_RUN_POOL_CHUNKS; it never drops below what
+// one query can need (n/2 runs) unless one of the two variables asks for less.  Buffers only
+// grow; the cap of a call is what it may use.
+int reserve_pool(Handle &H, int64_t m, int ns)
+{
+    const unsigned long long per_chunk = sizeof(uint2) * RUN_CHUNK + sizeof(int);
+    const unsigned long long min_chunks =
+        (unsigned long long)((H.n / 2 + 1 + RUN_CHUNK - 1) / RUN_CHUNK) + (unsigned long long)ns + 64;
+    unsigned long long want = (unsigned long long)m * 24ULL;
+    if (want < min_chunks) want = min_chunks;
+    const char *env = getenv("PB_RUN_POOL_MB");
+    const char *envc = getenv("PB_RUN_POOL_CHUNKS");
+    long long env_mb = env ? atoll(env) : 0, env_chunks = envc ? atoll(envc) : 0;
+    unsigned long long budget;
+    if (env_mb > 0) budget = (unsigned long long)env_mb << 20;
+    else {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        budget = tot / 6;
+        if (budget > (24ULL << 30)) budget = 24ULL << 30;
+    }
+    unsigned long long cap = budget / per_chunk;
+    if (cap > want) cap = want;
+    if (env_mb <= 0 && cap < min_chunks) cap = min_chunks;
+    if (env_chunks > 0) cap = (unsigned long long)env_chunks;
+    if (cap < 1) cap = 1;
+    if (cap > 0x7fffffffULL) cap = 0x7fffffffULL;
+    for (;;) {
+        cudaError_t e1 = H.pool_runs.reserve(sizeof(uint2) * RUN_CHUNK * cap);
+        cudaError_t e2 = e1 ? e1 : H.pool_next.reserve(sizeof(int) * cap);
+        if (e2 == cudaSuccess) break;
+        cudaGetLastError();
+        if (e2 != cudaErrorMemoryAllocation || cap / 2 < min_chunks)
+            return fail(H, PB_ERR_CUDA, std::string("run pool allocation failed: ") + cudaGetErrorString(e2));
+        H.pool_runs.release();
+        H.pool_next.release();
+        cap /= 2;
+    }
+    H.pool_cap = cap;
+    CK(H.pool_ctr.reserve(32));
+    CK(H.items.reserve(sizeof(int2) * m * ns));
+    CK(H.wbnear.reserve(sizeof(int) * m));
+    CK(H.qacc.reserve(sizeof(unsigned) * m));
+    CK(H.qflag.reserve(sizeof(int) * m));
+    CK(H.defer_a.reserve(sizeof(uint32_t) * m));
+    CK(H.defer_b.reserve(sizeof(uint32_t) * m));
+    return PB_OK;
+}
+
+// FP32-compensated points in two phases: the walk kernels write every (query, subtree) item's
+// accepted runs, the pair kernel evaluates them (once per catalog launch, heaviest queries
+// first).  Queries that found the pool full are walked again in another round with an
+// emptied pool; if a round completes none of its queries, the fused walk-and-sum kernel takes
+// the rest.  Both kernels produce identical bits for a query.
+int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &launches, std::vector<double *> &dev,
+                     int strategy, int64_t npts, const double *dx, const double *dy, const double *dz,
+                     const uint32_t *perm)
+{
+    if (npts > 0x7fffffffLL) return fail(H, PB_ERR_CAPACITY, "more than 2^31-1 sample points in one call");
+    int ns = 1;
+    CK(launch_cut(&H, T, H.walk_split, &ns));
+    int rc = reserve_pool(H, npts, ns);
+    if (rc) return rc;
+    const uint32_t *ql = perm;
+    if (!ql) {
+        CK(H.iota.reserve(sizeof(uint32_t) * npts));
+        CK(launch_iota(&H, npts, H.iota.as<uint32_t>()));
+        ql = H.iota.as<uint32_t>();
+    }
+    int64_t m = npts;
+    uint32_t *lists[2] = {H.defer_a.as<uint32_t>(), H.defer_b.as<uint32_t>()};
+    unsigned long long *ctr = H.pool_ctr.as<unsigned long long>();
+    H.walk_rounds = 0;
+    H.deferred_total = 0;
+    for (int round = 0;; ++round) {
+        CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
+        CK(cudaMemsetAsync(H.qacc.p, 0, sizeof(unsigned) * m, H.stream));
+        CK(cudaMemsetAsync(H.qflag.p, 0, sizeof(int) * m, H.stream));
+        RunPool P;
+        P.runs = H.pool_runs.as<uint2>();
+        P.next = H.pool_next.as<int>();
+        P.used = ctr;
+        P.cap = H.pool_cap;
+        P.ns = ns;
+        P.cut = H.cut.as<int2>() + (4 * H.walk_split + 8);
+        P.items = H.items.as<int2>();
+        P.bnear = H.wbnear.as<int>();
+        P.qacc = H.qacc.as<unsigned>();
+        P.qflag = H.qflag.as<int>();
+        P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
+        P.deferred = lists[round & 1];
+        if (strategy != SCATTER) {
+            CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
+            H.interp_launches++;
+        }
+        CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
+        H.interp_launches++;
+        uint32_t *order = nullptr;
+        CK(launch_lpt_order(&H, P, m, &order));
+        for (const Launch &Lc : launches) {
+            DevCatalog C = dev_catalog(H, Lc, dev.data());
+            CK(launch_pairs_fp32(&H, T, C, strategy, P, m, ql, order, dx, dy, dz));
+            H.interp_launches++;
+        }
+        unsigned nd = 0;
+        CK(cudaMemcpyAsync(&nd, P.n_deferred, sizeof(unsigned), cudaMemcpyDeviceToHost, H.stream));
+        CK(cudaStreamSynchronize(H.stream));
+        H.walk_rounds = round + 1;
+        if (nd == 0) break;
+        H.deferred_total += nd;
+        if ((int64_t)nd > m - m / 8) {   // under 1/8 of the queries completed: finish them fused
+            for (const Launch &Lc : launches) {
+                DevCatalog C = dev_catalog(H, Lc, dev.data());
+                CK(launch_points_fp32(&H, T, C, strategy, nd, dx, dy, dz, P.deferred, npts));
+                H.interp_launches++;
+            }
+            break;
+        }
+        ql = P.deferred;
+        m = nd;
+    }
+    return PB_OK;
+}
+
 int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, const double *qy,
               const double *qz, int32_t strategy, int32_t precision, double *const *out)
 {
@@ -428,11 +557,14 @@ int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, 
     DevTree T = make_tree(H);
     std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
     ev_record(H, 2);
-    for (const Launch &Lc : launches) {
-        DevCatalog C = dev_catalog(H, Lc, dev.data());
-        if (precision == PB_FP64) CK(launch_points_fp64(&H, T, C, strategy, npts, dx, dy, dz, perm));
-        else CK(launch_points_fp32(&H, T, C, strategy, npts, dx, dy, dz, perm));
-        H.interp_launches++;
+    if (precision == PB_FP64) {
+        for (const Launch &Lc : launches) {
+            DevCatalog C = dev_catalog(H, Lc, dev.data());
+            CK(launch_points_fp64(&H, T, C, strategy, npts, dx, dy, dz, perm));
+            H.interp_launches++;
+        }
+    } else if ((rc = two_phase_points(H, T, launches, dev, strategy, npts, dx, dy, dz, perm))) {
+        return rc;
     }
     ev_record(H, 3);
     if ((rc = finish_outputs(H, L, npts, out, dev, is_host))) return rc;
@@ -559,6 +691,10 @@ int32_t pb_set_option(pb_handle *h, const char *name, int64_t value)
     if (!strcmp(name, "timing")) H.timing = value != 0;
     else if (!strcmp(name, "sort_queries")) H.sort_queries = (int)value;
     else if (!strcmp(name, "block_size")) H.block_size = (int)value;
+    else if (!strcmp(name, "walk_split")) {
+        if (value < 1 || value > 4096) return fail(H, PB_ERR_INVALID, "walk_split must be in 1..4096");
+        H.walk_split = (int)value;
+    }
     else return fail(H, PB_ERR_INVALID, std::string("unknown option ") + name);
     return PB_OK;
 }
@@ -762,6 +898,15 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
 }
 
 int64_t pb_launch_count(const pb_handle *h) { return h ? h->H.launches : 0; }
+
+int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks)
+{
+    if (!h) return PB_ERR_INVALID;
+    if (walk_rounds) *walk_rounds = h->H.walk_rounds;
+    if (deferred) *deferred = h->H.deferred_total;
+    if (pool_chunks) *pool_chunks = (int64_t)h->H.pool_cap;
+    return PB_OK;
+}
 
 int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms, int64_t *interp_launches)
 {

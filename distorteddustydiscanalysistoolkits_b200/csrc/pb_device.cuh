@@ -56,6 +56,31 @@ struct DevTree {
     int *status;
 };
 
+// Accepted-neighbour run lists written by the walk kernel and read by the pair kernels.
+// The tree is cut into ns disjoint subtrees whose leaf ranges follow one another in DFS
+// order; every (query, subtree) item is walked separately.  A run is a maximal interval of
+// consecutive sorted leaves accepted by one item, stored as (first leaf, length); an item's
+// runs are kept in DFS (= ascending leaf) order in a linked list of fixed-size chunks drawn
+// from one pool, and items[j * ns + s] = (first chunk, number of runs).  Concatenating a
+// query's items in subtree order gives its accepted leaves in the reference's DFS order.
+constexpr int RUN_CHUNK = 32;
+constexpr int RUN_DEFERRED = -2;
+
+struct RunPool {
+    uint2 *runs;                  // cap * RUN_CHUNK (first leaf, length)
+    int *next;                    // cap chunk links (-1 ends a list)
+    unsigned long long *used;     // chunks handed out (may run past cap)
+    unsigned long long cap;       // chunks in the pool
+    int ns;                       // subtrees of the cut
+    const int2 *cut;              // (subtree root, node after the subtree in DFS order) per subtree
+    int2 *items;                  // m * ns item heads
+    int *bnear;                   // nearest sorted leaf per walked query (-1: none / not needed)
+    unsigned *qacc;               // accepted leaves per walked query
+    int *qflag;                   // 1: some item of the query found the pool full (deferred)
+    unsigned *n_deferred;         // queries deferred in this walk
+    uint32_t *deferred;           // their query indices
+};
+
 // Catalog of one launch.  ucol[] are the unique sorted quantity columns read per
 // neighbour; outputs index into them.  g_u == -1 is the density gradient (the
 // reference's grad slot 0, general_interpolation.jl:76-81).

@@ -66,6 +66,13 @@ struct Handle {
     std::vector<DBuf> cols_s;
     DBuf col_ptrs;      // device array of sorted column pointers
 
+    // run lists of the two-phase point path (walk kernel -> pair kernels)
+    DBuf pool_runs, pool_next, pool_ctr, items, wbnear, qacc, qflag, cut, defer_a, defer_b, lpt_k, lpt_v, lpt_ka,
+        lpt_va, iota;
+    int walk_split = 64;   // target number of subtrees each query's walk is split into
+    unsigned long long pool_cap = 0;
+    int64_t walk_rounds = 0, deferred_total = 0;
+
     // query-side scratch
     DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
     std::vector<DBuf> q_outs;
@@ -96,11 +103,24 @@ cudaError_t launch_query_codes(Handle *H, int64_t nq, const double *qx, const do
                                uint32_t *keys, uint32_t *perm);
 cudaError_t launch_permute_back(Handle *H, int64_t n, const uint32_t *idx, const double *src, double *dst);
 
+// ---- launchers (pb_walk.cu) ----
+cudaError_t launch_cut(Handle *H, const DevTree &T, int target, int *ns_out);
+cudaError_t launch_nearest_list(Handle *H, const DevTree &T, int64_t m, const uint32_t *ql, const double *qx,
+                                const double *qy, const double *qz, int *bnear);
+cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m, const uint32_t *ql,
+                        const double *qx, const double *qy, const double *qz, unsigned long long *counter);
+cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order);
+cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out);
+
 // ---- launchers (pb_interp64.cu / pb_interp32.cu / pb_query.cu) ----
+cudaError_t launch_pairs_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, const RunPool &P,
+                              int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                              const double *qy, const double *qz);
 cudaError_t launch_points_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
                                const double *qx, const double *qy, const double *qz, const uint32_t *perm);
 cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
-                               const double *qx, const double *qy, const double *qz, const uint32_t *perm);
+                               const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                               int64_t npts);
 cudaError_t launch_lines_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int64_t nl, const double *ox,
                               const double *oy, const double *oz, const double *dx, const double *dy,
                               const double *dz, const uint32_t *perm);

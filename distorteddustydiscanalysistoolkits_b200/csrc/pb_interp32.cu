@@ -324,11 +324,68 @@ __device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, con
     }
 }
 
+// per-query constants: kernel scale factors at h_a, the query position as double-float
+// pairs, and the quantity offsets (nearest particle, else the first accepted neighbour)
+template <int STRAT>
+__device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, double py, double pz, int64_t bnear,
+                                        Query32 &Q, Acc32 &A, const float4 *pay, int stride)
+{
+    Q = Query32{};
+    if (STRAT != SCATTER) {
+        double ha = bnear < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + bnear).w;
+        float ih = (float)(1.0 / ha);
+        Q.ih = ih;
+        Q.cw = sig * ih * ih * ih;
+        Q.cg = Q.cw * ih;
+    }
+    Q.ph[0] = (float)px; Q.pl[0] = (float)(px - (double)Q.ph[0]);
+    Q.ph[1] = (float)py; Q.pl[1] = (float)(py - (double)Q.ph[1]);
+    Q.ph[2] = (float)pz; Q.pl[2] = (float)(pz - (double)Q.ph[2]);
+    A.init();
+    if (bnear >= 0) {
+        // quantities enter as offsets from the nearest particle's values, which are close
+        // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
+        float cw_, cg_;
+        load_cols(pay + bnear * stride, stride, cw_, cg_, A.hh, A.hl);
+        A.have = true;
+    }
+}
+
+__device__ __forceinline__ void offsets_from(Acc32 &A, const float4 *pay, int stride, int64_t b0)
+{
+    float cw_, cg_;
+    load_cols(pay + b0 * stride, stride, cw_, cg_, A.hh, A.hl);
+    A.have = true;
+}
+
+// flush, fixed-tree FP64 reduction of the 32 lane sums, lane 0 finalises
+__device__ __forceinline__ void reduce_finalize32(Acc32 &A, const DevCatalog &C, bool need_grad, int64_t qi, int lane)
+{
+    A.flush(C, need_grad);
+    double v[15];
+    v[0] = A.S1.val();
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) v[1 + u] = A.SA[u].val();
+    v[5] = A.B[0].val(); v[6] = A.B[1].val(); v[7] = A.B[2].val();
+    v[8] = A.F[0][0].val(); v[9] = A.F[0][1].val(); v[10] = A.F[0][2].val();
+    v[11] = A.D[0].val();
+    v[12] = A.Cc[0][0].val(); v[13] = A.Cc[0][1].val(); v[14] = A.Cc[0][2].val();
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 15; ++a) v[a] += __shfl_down_sync(0xffffffffu, v[a], off);
+    }
+    if (lane == 0) finalize32w(v, A, C, qi);
+}
+
+// Fused form: the warp walks the query's tree itself (warp-uniform next_item) and deals the
+// accepted leaves to its lanes.  Used for queries the run pool could not hold.
 template <int STRAT, int KT>
 __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
                                                    int64_t nq, const double *__restrict__ qx,
                                                    const double *__restrict__ qy, const double *__restrict__ qz,
-                                                   const uint32_t *__restrict__ perm, unsigned long long *counter)
+                                                   const uint32_t *__restrict__ perm, int64_t npts,
+                                                   unsigned long long *counter)
 {
     const int lane = threadIdx.x & 31;
     const int64_t n = T.n;
@@ -339,39 +396,18 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         int64_t j = next_query(counter, lane);
         if (j >= nq) break;
         int64_t qi = perm ? (int64_t)__ldg(perm + j) : j;
-        if (qi >= nq) continue;
+        if (qi >= npts) continue;
         double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        int64_t bnear = STRAT != SCATTER ? nearest_leaf(T, px, py, pz) : -1;
         double ha = 0.0;
-        Query32 Q{};
-        int64_t bnear = -1;
-        if (STRAT != SCATTER) {
-            bnear = nearest_leaf(T, px, py, pz);
-            ha = bnear < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + bnear).w;
-            float ih = (float)(1.0 / ha);
-            Q.ih = ih;
-            Q.cw = sig * ih * ih * ih;
-            Q.cg = Q.cw * ih;
-        }
+        if (STRAT != SCATTER) ha = bnear < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + bnear).w;
         double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
-        Q.ph[0] = (float)px; Q.pl[0] = (float)(px - (double)Q.ph[0]);
-        Q.ph[1] = (float)py; Q.pl[1] = (float)(py - (double)Q.ph[1]);
-        Q.ph[2] = (float)pz; Q.pl[2] = (float)(pz - (double)Q.ph[2]);
+        Query32 Q;
         Acc32 A;
-        A.init();
-        float cw_, cg_;
-        if (bnear >= 0) {
-            // quantities enter as offsets from the nearest particle's values, which are close
-            // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
-            load_cols(pay + bnear * stride, stride, cw_, cg_, A.hh, A.hl);
-            A.have = true;
-        }
+        setup32<STRAT>(T, sig, px, py, pz, bnear, Q, A, pay, stride);
         Slots S{0, -1};
         auto proc = [&](int fill) {
-            if (!A.have) {
-                int64_t b0 = __shfl_sync(0xffffffffu, S.mine, 0);
-                load_cols(pay + b0 * stride, stride, cw_, cg_, A.hh, A.hl);
-                A.have = true;
-            }
+            if (!A.have) offsets_from(A, pay, stride, __shfl_sync(0xffffffffu, S.mine, 0));
             if (S.mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, S.mine);
         };
         if (T.root == 0) {
@@ -384,22 +420,90 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
             while (next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) deal(S, lane, lo, hi, proc);
         }
         if (S.fill > 0) proc(S.fill);
-        A.flush(C, need_grad);
-        // fixed-tree FP64 reduction of the 32 lane sums
-        double v[15];
-        v[0] = A.S1.val();
+        reduce_finalize32(A, C, need_grad, qi, lane);
+    }
+}
+
+// Pair kernel of the two-phase path: a warp takes a walked query (heaviest first), reads the
+// runs of its (query, subtree) items in subtree order, chunk by chunk, and deals the accepted
+// leaves to its lanes in DFS order -- the k-th accepted leaf to lane k mod 32, exactly as the
+// fused kernel does, so both produce the same bits.  Within a chunk, lane l finds the run
+// holding its leaf by a binary search over the inclusive prefix sums of the run lengths
+// held one per lane.
+template <int STRAT, int KT>
+__global__ void __launch_bounds__(128) k_pairs32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
+                                                  RunPool P, int64_t m, const uint32_t *__restrict__ ql,
+                                                  const uint32_t *__restrict__ order, const double *__restrict__ qx,
+                                                  const double *__restrict__ qy, const double *__restrict__ qz,
+                                                  unsigned long long *counter)
+{
+    const int lane = threadIdx.x & 31;
+    const float sig = ldexp_norm3(KT);
+    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
+    const int ns = P.ns;
+    for (;;) {
+        int64_t t = next_query(counter, lane);
+        if (t >= m) break;
+        const int64_t j = order ? (int64_t)__ldg(order + t) : t;
+        if (__ldg(P.qflag + j)) continue;
+        const int64_t qi = __ldg(ql + j);
+        const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        Query32 Q;
+        Acc32 A;
+        setup32<STRAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride);
+        int fill = 0;
+        int64_t mine = -1;
+        for (int s0 = 0; s0 < ns; s0 += 32) {
+            const int2 itm = s0 + lane < ns ? __ldg(P.items + j * ns + s0 + lane) : make_int2(-1, 0);
+            unsigned nonempty = __ballot_sync(0xffffffffu, itm.y > 0);
+            while (nonempty) {
+                const int l = __ffs(nonempty) - 1;
+                nonempty &= nonempty - 1;
+                int c = __shfl_sync(0xffffffffu, itm.x, l);
+                int left = __shfl_sync(0xffffffffu, itm.y, l);
+                if (!A.have) offsets_from(A, pay, stride, __ldg(&P.runs[(int64_t)c * RUN_CHUNK].x));
+                while (left > 0) {
+                    const int cnt = left < RUN_CHUNK ? left : RUN_CHUNK;
+                    const uint2 rn = lane < cnt ? __ldg(P.runs + (int64_t)c * RUN_CHUNK + lane) : make_uint2(0u, 0u);
+                    const int nextc = left > RUN_CHUNK ? __ldg(P.next + c) : -1;
+                    unsigned inc = rn.y;
 #pragma unroll
-        for (int u = 0; u < MAXU; ++u) v[1 + u] = A.SA[u].val();
-        v[5] = A.B[0].val(); v[6] = A.B[1].val(); v[7] = A.B[2].val();
-        v[8] = A.F[0][0].val(); v[9] = A.F[0][1].val(); v[10] = A.F[0][2].val();
-        v[11] = A.D[0].val();
-        v[12] = A.Cc[0][0].val(); v[13] = A.Cc[0][1].val(); v[14] = A.Cc[0][2].val();
+                    for (int o = 1; o < 32; o <<= 1) {
+                        unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+                        if (lane >= o) inc += v;
+                    }
+                    const int64_t tot = __shfl_sync(0xffffffffu, inc, 31);
+                    const unsigned ex_own = inc - rn.y;
+                    int64_t tb = -fill;
+                    for (;;) {
+                        const int64_t tl = tb + lane;
+                        const bool here = tl >= 0 && tl < tot;
+                        const unsigned tt = here ? (unsigned)tl : 0u;
+                        int r = 0;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-#pragma unroll
-            for (int a = 0; a < 15; ++a) v[a] += __shfl_down_sync(0xffffffffu, v[a], off);
+                        for (int sh = 16; sh > 0; sh >>= 1) {
+                            unsigned v = __shfl_sync(0xffffffffu, inc, r + sh - 1);
+                            if (v <= tt) r += sh;
+                        }
+                        const unsigned lo = __shfl_sync(0xffffffffu, rn.x, r);
+                        const unsigned ex = __shfl_sync(0xffffffffu, ex_own, r);
+                        if (here) mine = (int64_t)lo + (tt - ex);
+                        if (tb + 31 < tot) {
+                            if (mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);
+                            mine = -1;
+                            tb += 32;
+                        } else {
+                            fill = (int)(tot - tb);
+                            break;
+                        }
+                    }
+                    left -= cnt;
+                    c = nextc;
+                }
+            }
         }
-        if (lane == 0) finalize32w(v, A, C, qi);
+        if (mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);
+        reduce_finalize32(A, C, need_grad, qi, lane);
     }
 }
 
@@ -414,31 +518,32 @@ static int persistent_grid(const void *kern, int bs)
 
 template <int STRAT, int KT>
 static void launch_one(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride, int64_t nq,
-                       const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                       const double *qx, const double *qy, const double *qz, const uint32_t *perm, int64_t npts,
                        unsigned long long *ctr)
 {
     const int bs = 128;
     k_points32w<STRAT, KT><<<persistent_grid((const void *)k_points32w<STRAT, KT>, bs), bs, 0, H->stream>>>(
-        T, C, pay, stride, nq, qx, qy, qz, perm, ctr);
+        T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr);
 }
 
 template <int STRAT>
 static void launch_kt(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride, int64_t nq,
-                      const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                      const double *qx, const double *qy, const double *qz, const uint32_t *perm, int64_t npts,
                       unsigned long long *ctr)
 {
     switch (T.kernel) {
-    case 0: launch_one<STRAT, 0>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    case 1: launch_one<STRAT, 1>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    case 2: launch_one<STRAT, 2>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    case 3: launch_one<STRAT, 3>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    case 4: launch_one<STRAT, 4>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    default: launch_one<STRAT, 5>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case 0: launch_one<STRAT, 0>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    case 1: launch_one<STRAT, 1>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    case 2: launch_one<STRAT, 2>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    case 3: launch_one<STRAT, 3>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    case 4: launch_one<STRAT, 4>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    default: launch_one<STRAT, 5>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
     }
 }
 
 cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
-                               const double *qx, const double *qy, const double *qz, const uint32_t *perm)
+                               const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                               int64_t npts)
 {
     int stride = payload_stride(C.nU);
     cudaError_t e = H->payload.reserve(sizeof(float4) * stride * T.n);
@@ -450,9 +555,56 @@ cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C,
     k_payload<<<grid_for(T.n, 256), 256, 0, H->stream>>>(T.n, T, C, pay, stride);
     cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), H->stream);
     switch (strategy) {
-    case GATHER: launch_kt<GATHER>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    case SCATTER: launch_kt<SCATTER>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
-    default: launch_kt<SYMMETRIC>(H, T, C, pay, stride, nq, qx, qy, qz, perm, ctr); break;
+    case GATHER: launch_kt<GATHER>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    case SCATTER: launch_kt<SCATTER>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    default: launch_kt<SYMMETRIC>(H, T, C, pay, stride, nq, qx, qy, qz, perm, npts, ctr); break;
+    }
+    H->launches += 2;
+    return cudaGetLastError();
+}
+
+template <int STRAT, int KT>
+static void launch_pairs_one(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride,
+                             const RunPool &P, int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                             const double *qy, const double *qz, unsigned long long *ctr)
+{
+    const int bs = 128;
+    k_pairs32w<STRAT, KT><<<persistent_grid((const void *)k_pairs32w<STRAT, KT>, bs), bs, 0, H->stream>>>(
+        T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr);
+}
+
+template <int STRAT>
+static void launch_pairs_kt(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride,
+                            const RunPool &P, int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                            const double *qy, const double *qz, unsigned long long *ctr)
+{
+    switch (T.kernel) {
+    case 0: launch_pairs_one<STRAT, 0>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 1: launch_pairs_one<STRAT, 1>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 2: launch_pairs_one<STRAT, 2>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 3: launch_pairs_one<STRAT, 3>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 4: launch_pairs_one<STRAT, 4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    default: launch_pairs_one<STRAT, 5>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    }
+}
+
+cudaError_t launch_pairs_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, const RunPool &P,
+                              int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                              const double *qy, const double *qz)
+{
+    int stride = payload_stride(C.nU);
+    cudaError_t e = H->payload.reserve(sizeof(float4) * stride * T.n);
+    if (e) return e;
+    e = H->counter.reserve(sizeof(unsigned long long));
+    if (e) return e;
+    float4 *pay = H->payload.as<float4>();
+    unsigned long long *ctr = H->counter.as<unsigned long long>();
+    k_payload<<<grid_for(T.n, 256), 256, 0, H->stream>>>(T.n, T, C, pay, stride);
+    cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), H->stream);
+    switch (strategy) {
+    case GATHER: launch_pairs_kt<GATHER>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case SCATTER: launch_pairs_kt<SCATTER>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    default: launch_pairs_kt<SYMMETRIC>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     }
     H->launches += 2;
     return cudaGetLastError();

@@ -176,6 +176,7 @@ __device__ __forceinline__ double far_d2_box(double px, double py, double pz, co
 struct Walk {
     int node;
     int64_t cur, end, guard, limit;
+    int stop = 0;   // node where the walk ends: 0 for the whole tree, a subtree's escape target for a subtree
 };
 
 template <int STRAT>
@@ -241,8 +242,8 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
     const float r2a_up = __double2float_ru(r2a);
     const float bulk_lim = __fmul_rd(__double2float_rd(r2a), MARGIN_DN);
     for (;;) {
-        if (w.node == 0) return false;
-        if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.node = 0; return false; }
+        if (w.node == w.stop) return false;
+        if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.node = w.stop; return false; }
         const int node = w.node;
         if (node >= n) {
             int64_t b = node - n;

@@ -1,0 +1,287 @@
+// pb_walk.cu -- the traversal half of the two-phase point interpolation.
+//
+// 1. k_nearest_list: the nearest particle of every query (gather/symmetric strategies;
+//    LBVH_find_nearest_h, LinearBVHQueries.jl:118-140), one thread per query.
+// 2. k_cut_mark / k_cut_order: a cut of the tree into ns subtrees of at most ceil(n/ns_target)
+//    leaves each (every node whose subtree is small enough while its parent's is not),
+//    listed in DFS order.  Their leaf ranges partition 0..n-1 in ascending order.
+// 3. k_walk_items: one thread per (query, subtree) item.  A warp walks one subtree for 32
+//    consecutive queries of the (Morton-ordered) list, so its lanes follow nearby paths, and
+//    a heavy query is spread over ns independent walks.  The walk is next_item<STRAT> of
+//    pb_interp_impl.cuh (the reference's acceptance predicate,
+//    LinearBVHTraversalMacros.jl:26-371) started at the subtree root and stopped at the node
+//    that follows the subtree in DFS order; accepted leaves are emitted as runs of consecutive
+//    sorted indices into a chunked pool.
+// The pair kernels read a query's items in subtree order, which is the reference's DFS order
+// of its accepted leaves.
+#include <cooperative_groups.h>
+
+#include "pb_internal.h"
+#include "pb_interp_impl.cuh"
+
+namespace pb {
+
+namespace cg = cooperative_groups;
+
+__global__ void __launch_bounds__(128) k_nearest_list(DevTree T, int64_t m, const uint32_t *__restrict__ ql,
+                                                      const double *__restrict__ qx, const double *__restrict__ qy,
+                                                      const double *__restrict__ qz, int *bnear)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t qi = __ldg(ql + j);
+        bnear[j] = (int)nearest_leaf(T, __ldg(qx + qi), __ldg(qy + qi), __ldg(qz + qi));
+    }
+}
+
+__device__ __forceinline__ int64_t subtree_size(const DevTree &T, int id)
+{
+    if (id >= T.n) return 1;
+    int2 r = __ldg(T.range + (id - 1));
+    return (int64_t)r.y - r.x + 1;
+}
+
+// cut nodes: size <= tsz < size(parent) (the root alone when n <= tsz)
+__global__ void k_cut_mark(DevTree T, const int *__restrict__ parent, int64_t tsz, int2 *cut, int *count, int cap)
+{
+    const int64_t ntot = T.root ? 2 * T.n - 1 : 1;
+    for (int64_t id = 1 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id <= ntot;
+         id += (int64_t)gridDim.x * blockDim.x) {
+        if (subtree_size(T, (int)id) > tsz) continue;
+        const int p = T.root ? parent[id - 1] : 0;
+        if (p != 0 && subtree_size(T, p) <= tsz) continue;
+        const int stop = id >= T.n ? __ldg(T.leaf_escape + (id - T.n)) : T.node[id - 1].escape;
+        int k = atomicAdd(count, 1);
+        if (k < cap) cut[k] = make_int2((int)id, stop);
+    }
+}
+
+// one block: order the cut nodes by the first sorted leaf of their subtrees (rank sort)
+__global__ void k_cut_order(DevTree T, const int2 *__restrict__ in, const int *count, int cap, int2 *out)
+{
+    const int k = min(*count, cap);
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        const int2 a = in[i];
+        const int la = a.x >= T.n ? (int)(a.x - T.n) : T.range[a.x - 1].x;
+        int rank = 0;
+        for (int t = 0; t < k; ++t) {
+            const int2 b = in[t];
+            const int lb = b.x >= T.n ? (int)(b.x - T.n) : T.range[b.x - 1].x;
+            rank += lb < la;
+        }
+        out[rank] = a;
+    }
+}
+
+// one chunk per calling thread; threads that arrive together share one atomic
+__device__ __forceinline__ int alloc_chunk(const RunPool &P)
+{
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(P.used, (unsigned long long)g.size());
+    base = g.shfl(base, 0);
+    unsigned long long c = base + g.thread_rank();
+    return c < P.cap ? (int)c : -1;
+}
+
+struct RunWriter {
+    int first = -1, cur = -1, k = 0;
+    int nruns = 0;
+    int64_t nacc = 0;
+    int64_t olo = -1, ohi = -1;   // open run
+
+    __device__ __forceinline__ bool store(const RunPool &P)
+    {
+        if (cur < 0 || k == RUN_CHUNK) {
+            int c = alloc_chunk(P);
+            if (c < 0) return false;
+            P.next[c] = -1;
+            if (cur >= 0) P.next[cur] = c;
+            else first = c;
+            cur = c;
+            k = 0;
+        }
+        P.runs[(int64_t)cur * RUN_CHUNK + k] = make_uint2((unsigned)olo, (unsigned)(ohi - olo + 1));
+        ++k;
+        ++nruns;
+        return true;
+    }
+    __device__ __forceinline__ bool emit(const RunPool &P, int64_t lo, int64_t hi)
+    {
+        nacc += hi - lo + 1;
+        if (olo >= 0 && lo == ohi + 1) {
+            ohi = hi;
+            return true;
+        }
+        bool ok = olo < 0 || store(P);
+        olo = lo;
+        ohi = hi;
+        return ok;
+    }
+    __device__ __forceinline__ bool close(const RunPool &P) { return olo < 0 || store(P); }
+};
+
+// warp items: (block of 32 list positions, subtree), query blocks outermost
+template <int STRAT>
+__global__ void __launch_bounds__(128) k_walk_items(DevTree T, RunPool P, int64_t m, const uint32_t *__restrict__ ql,
+                                                    const double *__restrict__ qx, const double *__restrict__ qy,
+                                                    const double *__restrict__ qz, unsigned long long *counter)
+{
+    const int lane = threadIdx.x & 31;
+    const int ns = P.ns;
+    const int64_t nitems = ((m + 31) / 32) * ns;
+    const double K = kernel_valid(T.kernel);
+    for (;;) {
+        unsigned long long wi = 0;
+        if (lane == 0) wi = atomicAdd(counter, 1ULL);
+        wi = __shfl_sync(0xffffffffu, wi, 0);
+        if ((int64_t)wi >= nitems) break;
+        const int64_t j = (int64_t)(wi / ns) * 32 + lane;
+        const int s = (int)(wi % ns);
+        if (j >= m) continue;
+        const uint32_t qi = __ldg(ql + j);
+        bool ok = *(volatile unsigned long long *)P.used < P.cap &&
+                  *(volatile int *)(P.qflag + j) == 0;   // pool exhausted or query already deferred
+        RunWriter R;
+        if (ok) {
+            const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+            double ha = 0.0;
+            if (STRAT != SCATTER) {
+                const int b = P.bnear[j];
+                ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
+            }
+            const double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
+            if (T.root == 0) {
+                double4 L;
+                double d2;
+                if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2)) ok = R.emit(P, 0, 0);
+            } else {
+                const int2 c = __ldg(P.cut + s);
+                Walk w{c.x, 1, 0, 0, 4 * T.n + 64, c.y};
+                int64_t lo, hi;
+                while (ok && next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) ok = R.emit(P, lo, hi);
+            }
+            if (ok) ok = R.close(P);
+        }
+        const int64_t it = j * ns + s;
+        if (!ok) {
+            P.items[it] = make_int2(RUN_DEFERRED, 0);
+            if (atomicExch(P.qflag + j, 1) == 0) {
+                unsigned d = atomicAdd(P.n_deferred, 1u);
+                P.deferred[d] = qi;
+            }
+            continue;
+        }
+        P.items[it] = make_int2(R.first, R.nruns);
+        if (R.nacc > 0) atomicAdd(P.qacc + j, (unsigned)R.nacc);
+    }
+}
+
+// descending accepted count first (deferred queries last): the heaviest queries start first
+__global__ void k_lpt_keys(int64_t m, const unsigned *__restrict__ qacc, const int *__restrict__ qflag,
+                           uint32_t *keys, uint32_t *vals)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+        unsigned a = qflag[j] ? 0u : qacc[j];
+        keys[j] = 0x7fffffffu - (a > 0x7fffffffu ? 0x7fffffffu : a);
+        vals[j] = (uint32_t)j;
+    }
+}
+
+__global__ void k_iota(int64_t m, uint32_t *out)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x)
+        out[j] = (uint32_t)j;
+}
+
+static int persistent_blocks(const void *kern, int bs)
+{
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, bs, 0);
+    return sms * (per > 0 ? per : 1);
+}
+
+cudaError_t launch_cut(Handle *H, const DevTree &T, int target, int *ns_out)
+{
+    const int64_t n = T.n;
+    int64_t tsz = (n + target - 1) / target;
+    if (tsz < 1) tsz = 1;
+    const int cap = 4 * target + 8;
+    cudaError_t e;
+    if ((e = H->cut.reserve(sizeof(int2) * 2 * cap + 16))) return e;
+    int2 *raw = H->cut.as<int2>();
+    int2 *sorted = raw + cap;
+    int *count = reinterpret_cast<int *>(raw + 2 * cap);
+    if ((e = cudaMemsetAsync(count, 0, sizeof(int), H->stream))) return e;
+    const int64_t ntot = T.root ? 2 * n - 1 : 1;
+    k_cut_mark<<<grid_for(ntot, 256), 256, 0, H->stream>>>(T, H->parent.as<int>(), tsz, raw, count, cap);
+    k_cut_order<<<1, 1024, 0, H->stream>>>(T, raw, count, cap, sorted);
+    H->launches += 2;
+    if ((e = cudaGetLastError())) return e;
+    int k = 0;
+    if ((e = cudaMemcpyAsync(&k, count, sizeof(int), cudaMemcpyDeviceToHost, H->stream))) return e;
+    if ((e = cudaStreamSynchronize(H->stream))) return e;
+    if (k < 1 || k > cap) return cudaErrorInvalidValue;
+    *ns_out = k;
+    return cudaSuccess;
+}
+
+cudaError_t launch_nearest_list(Handle *H, const DevTree &T, int64_t m, const uint32_t *ql, const double *qx,
+                                const double *qy, const double *qz, int *bnear)
+{
+    k_nearest_list<<<grid_for(m, 128, 1 << 30), 128, 0, H->stream>>>(T, m, ql, qx, qy, qz, bnear);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m, const uint32_t *ql,
+                        const double *qx, const double *qy, const double *qz, unsigned long long *counter)
+{
+    const int bs = 128;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), H->stream);
+    if (e) return e;
+    switch (strategy) {
+    case GATHER:
+        k_walk_items<GATHER><<<persistent_blocks((const void *)k_walk_items<GATHER>, bs), bs, 0, H->stream>>>(
+            T, P, m, ql, qx, qy, qz, counter);
+        break;
+    case SCATTER:
+        k_walk_items<SCATTER><<<persistent_blocks((const void *)k_walk_items<SCATTER>, bs), bs, 0, H->stream>>>(
+            T, P, m, ql, qx, qy, qz, counter);
+        break;
+    default:
+        k_walk_items<SYMMETRIC><<<persistent_blocks((const void *)k_walk_items<SYMMETRIC>, bs), bs, 0, H->stream>>>(
+            T, P, m, ql, qx, qy, qz, counter);
+        break;
+    }
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order)
+{
+    cudaError_t e;
+    if ((e = H->lpt_k.reserve(4 * m))) return e;
+    if ((e = H->lpt_v.reserve(4 * m))) return e;
+    if ((e = H->lpt_ka.reserve(4 * m))) return e;
+    if ((e = H->lpt_va.reserve(4 * m))) return e;
+    k_lpt_keys<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, H->lpt_k.as<uint32_t>(),
+                                                        H->lpt_v.as<uint32_t>());
+    H->launches += 1;
+    if ((e = cudaGetLastError())) return e;
+    if ((e = sort_pairs_u32(H, H->lpt_k.as<uint32_t>(), H->lpt_v.as<uint32_t>(), H->lpt_ka.as<uint32_t>(),
+                            H->lpt_va.as<uint32_t>(), m, 31)))
+        return e;
+    *order = H->lpt_v.as<uint32_t>();
+    return cudaSuccess;
+}
+
+cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out)
+{
+    k_iota<<<grid_for(m, 256), 256, 0, H->stream>>>(m, out);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace pb

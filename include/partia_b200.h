@@ -79,7 +79,8 @@ int32_t pb_last_error(const pb_handle *h, char *buf, int64_t size);
 /* Launch on this stream (a cudaStream_t of the handle's device); NULL = the handle's own. */
 int32_t pb_set_stream(pb_handle *h, void *cuda_stream);
 /* Options: "timing" (record CUDA events around build/traversal), "sort_queries"
-   (Morton-order queries before traversal; schedule only), "block_size". */
+   (Morton-order queries before traversal; schedule only), "block_size", "walk_split" (target
+   number of subtrees each FP32-compensated point walk is split into, 1..4096; schedule only). */
 int32_t pb_set_option(pb_handle *h, const char *name, int64_t value);
 
 /* LinearBVH!(input, Val(3)) (InterpolationInput.jl:203-223): MortonEncoding
@@ -166,6 +167,12 @@ int32_t pb_morton_sort_noalloc(const double *x, const double *y, const double *z
    the last call in ms (needs option "timing"); traversal kernel launches of the last call. */
 int64_t pb_launch_count(const pb_handle *h);
 int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms, int64_t *interp_launches);
+
+/* Diagnostics of the last FP32-compensated point call (no counterpart in the reference):
+   walk rounds taken, queries deferred because the accepted-run pool was full (they are walked
+   again, or finished by the fused kernel), and the pool size in chunks of 32 runs.  The pool
+   follows PB_RUN_POOL_MB (MiB) or PB_RUN_POOL_CHUNKS from the environment when set. */
+int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks);
 
 #ifdef __cplusplus
 }
