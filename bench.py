@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-roofline", action="store_true", help="skip the event-count pass (profiling runs)")
     ap.add_argument("--json-out", default=None)
     return ap.parse_args()
 
@@ -131,10 +132,12 @@ class ClockSampler:
 
 
 def algorithmic_bytes(stats, L, k_cols, s):
-    """Reference-algorithm bytes of one traversal launch over all queries (see module doc)."""
+    """Reference-algorithm bytes of the two kernel phases over all queries (see module doc):
+    the traversal (nearest search + walk: query points and tree visits) and the pair sums
+    (per accepted neighbour m, rho and k quantity columns at s bytes, per query L outputs)."""
     nv, nl, mv, ml, acc = (stats[:, i].astype(np.float64).sum() for i in range(5))
     nq = stats.shape[0]
-    return nq * (24 + 8 * L) + 32 * nv + 24 * nl + 36 * mv + 28 * ml + acc * (2 + k_cols) * s
+    return {"walk": nq * 24 + 32 * nv + 24 * nl + 36 * mv + 28 * ml, "pairs": nq * 8 * L + acc * (2 + k_cols) * s}
 
 
 def cpu_baseline(p, flat, cols, cat, seconds):
@@ -245,7 +248,10 @@ def main():
                                                   qp[2], pb.itpSymmetric.code, pcode, optrs, 0)
         H.check(rc, "pb_point_samples_interpolation")
         b, i, nl = H.timings()
+        phases.append(H.phase_times())
         return b, i
+
+    phases = []
 
     flush = torch.empty(L2_FLUSH_BYTES // 8, dtype=torch.float64, device="cuda")
     for _ in range(args.warmup):
@@ -258,6 +264,7 @@ def main():
         torch.distributed.barrier()
     launches0 = H.launch_count()
     builds, interps = [], []
+    phases.clear()
     for _ in range(args.steps):
         flush.zero_()            # L2 flush between timed steps, outside the per-step events
         b, i = step()
@@ -272,25 +279,42 @@ def main():
     build_ms, interp_ms, step_ms = _max_over_ranks([build_ms, interp_ms, build_ms + interp_ms], world)
     value = world * npts / (interp_ms / 1e3)
 
-    # roofline of the traversal kernel (one launch per step for this catalog)
+    # roofline of the dominant kernel phase (FP32C: walk kernels vs pair kernel, per-phase CUDA
+    # events of the library; FP64: the fused kernel)
     lb = pb.LinearBVH(backend, args.particles)
-    stats = pb.traversal_stats(lb, [c.cpu().numpy() for c in q], pb.itpSymmetric)
-    s = 4 if prec == pb.FP32C else 8
-    alg_bytes = algorithmic_bytes(stats, cat.L, len(cols), s)
-    peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(REPO, "MEASURED_PEAKS.json")) else None
-    peak = peaks["hbm_gbs"] if peaks else 6650.0
-    achieved = alg_bytes / (interp_ms / 1e3) / 1e9
-    traffic = None
-    prof = os.path.join(REPO, "profiles", "k_points_fp32c_symmetric_c2.json")
-    if os.path.exists(prof) and args.precision == "fp32c" and args.particles == (1 << 21):
-        traffic = json.load(open(prof)).get("dram_bytes_per_launch")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_points<Comp32,itpSymmetric>" if s == 4 else "k_points<Exact64,itpSymmetric>",
-                "algorithmic_bytes_per_launch": alg_bytes,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
-                "events_per_query": {k: float(stats[:, i].mean()) for i, k in enumerate(
-                    ("nearest_internal", "nearest_leaf", "main_internal", "main_leaf", "accepted"))}}
+    roofline = None
+    if not args.no_roofline:
+        stats = pb.traversal_stats(lb, [c.cpu().numpy() for c in q], pb.itpSymmetric)
+        s = 4 if prec == pb.FP32C else 8
+        alg = algorithmic_bytes(stats, cat.L, len(cols), s)
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(REPO, "MEASURED_PEAKS.json")) else None
+        peak = peaks["hbm_gbs"] if peaks else 6650.0
+        ph = np.mean(np.array(phases), axis=0) if phases else np.zeros(3)
+        if prec == pb.FP32C:
+            kern = {"walk": ("k_nearest_list + k_walk_items<itpSymmetric>", ph[0] + ph[1]),
+                    "pairs": ("k_pairs32w<itpSymmetric,M4>", ph[2])}
+        else:
+            kern = {"fused": ("k_points64w<itpSymmetric>", interp_ms)}
+            alg = {"fused": alg["walk"] + alg["pairs"]}
+        per = {}
+        for key, (name, ms) in kern.items():
+            a = alg[key] / (ms / 1e3) / 1e9 if ms > 0 else None
+            per[key] = {"kernel": name, "ms": float(ms), "algorithmic_bytes": alg[key], "achieved_gbs": a}
+        dom = max(per, key=lambda k: per[k]["ms"])
+        traffic = None
+        prof = os.path.join(REPO, "profiles", "%s_c2_traffic.json" % dom)
+        if os.path.exists(prof) and args.precision == "fp32c" and args.particles == (1 << 21) and \
+                args.grid == "256,256,64":
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        achieved = per[dom]["achieved_gbs"]
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak if achieved else None, "traffic": traffic,
+                    "kernel": per[dom]["kernel"], "algorithmic_bytes_per_launch": alg[dom],
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
+                    "phases": per,
+                    "events_per_query": {k: float(stats[:, i].mean()) for i, k in enumerate(
+                        ("nearest_internal", "nearest_leaf", "main_internal", "main_leaf", "accepted"))}}
 
     # accuracy of the FP32-compensated fields against the FP64 path (bit-exact to the oracle)
     accuracy = None

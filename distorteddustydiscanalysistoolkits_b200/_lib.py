@@ -100,7 +100,7 @@ def load():
                                           [_vp] * 6 + [ctypes.c_int32, ctypes.c_int32, P(_vp), ctypes.c_int32]),
         "pb_launch_count": (ctypes.c_int64, [_vp]),
         "pb_last_timings": (ctypes.c_int32, [_vp, _dp, _dp, _lp]),
-        "pb_last_schedule": (ctypes.c_int32, [_vp, _lp, _lp, _lp]),
+        "pb_last_schedule": (ctypes.c_int32, [_vp, _lp, _lp, _lp, _dp]),
         "pb_morton_sort_noalloc": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
@@ -185,5 +185,11 @@ class Handle:
     def schedule(self):
         """(walk rounds, deferred queries, pool chunks) of the last FP32-compensated point call."""
         r, d, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
-        self.lib.pb_last_schedule(self.h, ctypes.byref(r), ctypes.byref(d), ctypes.byref(c))
+        self.lib.pb_last_schedule(self.h, ctypes.byref(r), ctypes.byref(d), ctypes.byref(c), None)
         return r.value, d.value, c.value
+
+    def phase_times(self):
+        """Device ms of the first round's nearest search, walk and pair sums (option "timing")."""
+        t = (ctypes.c_double * 3)()
+        self.lib.pb_last_schedule(self.h, None, None, None, t)
+        return tuple(t)

@@ -183,10 +183,52 @@ std::vector<Item> items_of(const pb_catalog *c, bool fp32)
 }
 
 struct Launch {
-    std::vector<int> ucols;
+    std::vector<int> ucols;   // column of each slot u
     std::vector<Item> items;
     int cnt[4] = {0, 0, 0, 0};
 };
+
+constexpr int PB_COL_NONE = -100;
+
+// Fixed slot layout of a launch: the gradient's column in slot 0, the divergence/curl vector
+// in slots 1..3 (one vector per launch), scalars in the slots left over or in the slot that
+// already holds their column.  The pair kernels then read every term's operands from fixed
+// slots.  Returns false when the items do not fit MAXU slots.
+bool layout(const std::vector<Item> &items, std::vector<int> &slots)
+{
+    std::vector<int> u(MAXU, PB_COL_NONE);
+    bool vec = false;
+    for (const Item &x : items) {
+        if (x.kind == 1 && x.ncols > 0) {
+            if (u[0] != PB_COL_NONE && u[0] != x.cols[0]) return false;
+            u[0] = x.cols[0];
+        }
+        if (x.kind >= 2) {
+            for (int d = 0; d < 3; ++d) {
+                if (u[1 + d] != PB_COL_NONE && u[1 + d] != x.cols[d]) return false;
+                u[1 + d] = x.cols[d];
+            }
+            vec = true;
+        }
+    }
+    for (const Item &x : items) {
+        if (x.kind != 0) continue;
+        if (std::find(u.begin(), u.end(), x.cols[0]) != u.end()) continue;
+        auto it = std::find(u.begin(), u.end(), PB_COL_NONE);
+        if (it == u.end()) return false;
+        *it = x.cols[0];
+    }
+    // slot 0 is read whenever a vector is present: it then holds a real column
+    if (vec && u[0] == PB_COL_NONE) u[0] = u[1];
+    int used = 0;
+    for (int k = 0; k < MAXU; ++k)
+        if (u[k] != PB_COL_NONE) used = k + 1;
+    for (int k = 0; k < used; ++k)
+        if (u[k] == PB_COL_NONE) u[k] = u[0] != PB_COL_NONE ? u[0] : u[1];
+    u.resize(used);
+    slots = u;
+    return true;
+}
 
 std::vector<Launch> plan(const std::vector<Item> &items)
 {
@@ -194,16 +236,15 @@ std::vector<Launch> plan(const std::vector<Item> &items)
     std::vector<Launch> out;
     Launch cur;
     for (const Item &x : items) {
-        std::vector<int> u = cur.ucols;
-        for (int k = 0; k < x.ncols; ++k)
-            if (std::find(u.begin(), u.end(), x.cols[k]) == u.end()) u.push_back(x.cols[k]);
-        bool fits = (int)u.size() <= MAXU && cur.cnt[x.kind] < lim[x.kind];
+        std::vector<Item> trial = cur.items;
+        trial.push_back(x);
+        std::vector<int> u;
+        bool fits = cur.cnt[x.kind] < lim[x.kind] && layout(trial, u);
         if (!fits) {
             out.push_back(cur);
             cur = Launch();
-            u.clear();
-            for (int k = 0; k < x.ncols; ++k)
-                if (std::find(u.begin(), u.end(), x.cols[k]) == u.end()) u.push_back(x.cols[k]);
+            trial.assign(1, x);
+            layout(trial, u);
         }
         cur.ucols = u;
         cur.items.push_back(x);
@@ -240,15 +281,15 @@ DevCatalog dev_catalog(Handle &H, const Launch &L, double *const *outs)
                 C.n_scalar++;
                 C.out[l++] = outs[x.out0];
             } else if (kind == 1) {
-                C.g_u[C.n_grad] = x.cols[0] == -1 ? -1 : uidx(L, x.cols[0]);
+                C.g_u[C.n_grad] = x.cols[0] == -1 ? -1 : 0;
                 C.n_grad++;
                 for (int d = 0; d < 3; ++d) C.out[l++] = outs[x.out0 + d];
             } else if (kind == 2) {
-                for (int d = 0; d < 3; ++d) C.d_u[C.n_div][d] = uidx(L, x.cols[d]);
+                for (int d = 0; d < 3; ++d) C.d_u[C.n_div][d] = 1 + d;
                 C.n_div++;
                 C.out[l++] = outs[x.out0];
             } else {
-                for (int d = 0; d < 3; ++d) C.c_u[C.n_curl][d] = uidx(L, x.cols[d]);
+                for (int d = 0; d < 3; ++d) C.c_u[C.n_curl][d] = 1 + d;
                 C.n_curl++;
                 for (int d = 0; d < 3; ++d) C.out[l++] = outs[x.out0 + d];
             }
@@ -498,22 +539,28 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
         P.qflag = H.qflag.as<int>();
         P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
         P.deferred = lists[round & 1];
+        if (round == 0) ev_record(H, 4);
         if (strategy != SCATTER) {
             CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
             H.interp_launches++;
         }
+        if (round == 0) ev_record(H, 5);
         CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
         H.interp_launches++;
         uint32_t *order = nullptr;
         CK(launch_lpt_order(&H, P, m, &order));
+        if (round == 0) ev_record(H, 6);
         for (const Launch &Lc : launches) {
             DevCatalog C = dev_catalog(H, Lc, dev.data());
             CK(launch_pairs_fp32(&H, T, C, strategy, P, m, ql, order, dx, dy, dz));
             H.interp_launches++;
         }
+        if (round == 0) ev_record(H, 7);
         unsigned nd = 0;
         CK(cudaMemcpyAsync(&nd, P.n_deferred, sizeof(unsigned), cudaMemcpyDeviceToHost, H.stream));
         CK(cudaStreamSynchronize(H.stream));
+        if (round == 0)
+            for (int k = 0; k < 3; ++k) H.t_phase_ms[k] = ev_ms(H, 4 + k, 5 + k);
         H.walk_rounds = round + 1;
         if (nd == 0) break;
         H.deferred_total += nd;
@@ -899,9 +946,12 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
 
 int64_t pb_launch_count(const pb_handle *h) { return h ? h->H.launches : 0; }
 
-int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks)
+int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks,
+                         double *phase_ms)
 {
     if (!h) return PB_ERR_INVALID;
+    if (phase_ms)
+        for (int k = 0; k < 3; ++k) phase_ms[k] = h->H.t_phase_ms[k];
     if (walk_rounds) *walk_rounds = h->H.walk_rounds;
     if (deferred) *deferred = h->H.deferred_total;
     if (pool_chunks) *pool_chunks = (int64_t)h->H.pool_cap;

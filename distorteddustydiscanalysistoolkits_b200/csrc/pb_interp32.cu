@@ -252,28 +252,16 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_
         float gq = mrho * G;
         float gx = gq * dx, gy = gq * dy, gz = gq * dz;
         A.pB[0] += gx; A.pB[1] += gy; A.pB[2] += gz;
-#pragma unroll
-        for (int j = 0; j < MAXG; ++j) {
-            if (j < C.n_grad) {
-                float av = pick<MAXU>(a, C.g_u[j]);
-                A.pF[j][0] += gx * av; A.pF[j][1] += gy * av; A.pF[j][2] += gz * av;
-            }
+        // fixed slots: the gradient's column in slot 0, the div/curl vector in slots 1..3
+        if (C.n_grad > 0) {
+            const float av = a[0];
+            A.pF[0][0] += gx * av; A.pF[0][1] += gy * av; A.pF[0][2] += gz * av;
         }
-#pragma unroll
-        for (int j = 0; j < MAXD; ++j) {
-            if (j < C.n_div) {
-                float ax = pick<MAXU>(a, C.d_u[j][0]), ay = pick<MAXU>(a, C.d_u[j][1]), az = pick<MAXU>(a, C.d_u[j][2]);
-                A.pD[j] += gx * ax + gy * ay + gz * az;
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < MAXC; ++j) {
-            if (j < C.n_curl) {
-                float ax = pick<MAXU>(a, C.c_u[j][0]), ay = pick<MAXU>(a, C.c_u[j][1]), az = pick<MAXU>(a, C.c_u[j][2]);
-                A.pC[j][0] += ay * gz - az * gy;
-                A.pC[j][1] += az * gx - ax * gz;
-                A.pC[j][2] += ax * gy - ay * gx;
-            }
+        if (C.n_div > 0) A.pD[0] += gx * a[1] + gy * a[2] + gz * a[3];
+        if (C.n_curl > 0) {
+            A.pC[0][0] += a[2] * gz - a[3] * gy;
+            A.pC[0][1] += a[3] * gx - a[1] * gz;
+            A.pC[0][2] += a[1] * gy - a[2] * gx;
         }
     }
     if (++A.cnt == CHUNK) A.flush(C, need_grad);
@@ -475,19 +463,38 @@ __global__ void __launch_bounds__(128) k_pairs32w(DevTree T, DevCatalog C, const
                     const int64_t tot = __shfl_sync(0xffffffffu, inc, 31);
                     const unsigned ex_own = inc - rn.y;
                     int64_t tb = -fill;
+                    // uniform cursor: run r0 holds leaf position max(tb, 0) of the chunk; a batch
+                    // inside one run needs no search
+                    int r0 = -1, rc = -1;
+                    unsigned end0 = 0, lo0 = 0, ex0 = 0;
                     for (;;) {
-                        const int64_t tl = tb + lane;
-                        const bool here = tl >= 0 && tl < tot;
-                        const unsigned tt = here ? (unsigned)tl : 0u;
-                        int r = 0;
-#pragma unroll
-                        for (int sh = 16; sh > 0; sh >>= 1) {
-                            unsigned v = __shfl_sync(0xffffffffu, inc, r + sh - 1);
-                            if (v <= tt) r += sh;
+                        // t0 < tot = inc[cnt - 1], so the cursor stops at a run of this chunk
+                        const unsigned t0 = tb <= 0 ? 0u : (tb < tot ? (unsigned)tb : (unsigned)(tot - 1));
+                        while (end0 <= t0 && r0 < 31) {
+                            ++r0;
+                            end0 = __shfl_sync(0xffffffffu, inc, r0);
                         }
-                        const unsigned lo = __shfl_sync(0xffffffffu, rn.x, r);
-                        const unsigned ex = __shfl_sync(0xffffffffu, ex_own, r);
-                        if (here) mine = (int64_t)lo + (tt - ex);
+                        if (tb >= 0 && tb + 32 <= (int64_t)end0) {
+                            if (rc != r0) {
+                                lo0 = __shfl_sync(0xffffffffu, rn.x, r0);
+                                ex0 = __shfl_sync(0xffffffffu, ex_own, r0);
+                                rc = r0;
+                            }
+                            mine = (int64_t)lo0 + ((unsigned)tb - ex0) + lane;
+                        } else {
+                            const int64_t tl = tb + lane;
+                            const bool here = tl >= 0 && tl < tot;
+                            const unsigned tt = here ? (unsigned)tl : 0u;
+                            int r = 0;
+#pragma unroll
+                            for (int sh = 16; sh > 0; sh >>= 1) {
+                                unsigned v = __shfl_sync(0xffffffffu, inc, r + sh - 1);
+                                if (v <= tt) r += sh;
+                            }
+                            const unsigned lo = __shfl_sync(0xffffffffu, rn.x, r);
+                            const unsigned ex = __shfl_sync(0xffffffffu, ex_own, r);
+                            if (here) mine = (int64_t)lo + (tt - ex);
+                        }
                         if (tb + 31 < tot) {
                             if (mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);
                             mine = -1;
