@@ -12,8 +12,8 @@
 //   * every quantity enters as an offset A_b - A_hat (A_hat = the nearest particle's value,
 //     or the first accepted neighbour's for scatter, as a double-float) so that
 //     gradient/divergence/curl F - A B cancels as little as possible;
-//   * sums are accumulated per chunk of 4 accepted pairs in plain FP32 and each chunk sum
-//     is folded into a TwoSum-compensated accumulator.
+//   * each lane sums its terms in plain FP32 over chunks of 4 full batches of 32 pairs (4 of
+//     its own pairs) and adds each chunk sum, converted exactly, to an FP64 accumulator.
 // The per-query arithmetic depends only on the query and the tree (chunks are counted over
 // the query's own accepted-neighbour sequence), never on the launch shape or schedule.
 #include "line_tables.h"
@@ -124,11 +124,19 @@ __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int s
     }
 }
 
+// FP64 accumulator of FP32 chunk sums: the conversion is exact and the FP64 additions carry
+// 29 more bits than the terms, so the chunk sums are the only FP32 rounding left
+struct DSum {
+    double d;
+    __device__ __forceinline__ void zero() { d = 0.0; }
+    __device__ __forceinline__ void add(float x) { d = __dadd_rn(d, (double)x); }
+    __device__ __forceinline__ double val() const { return d; }
+};
+
 struct Acc32 {
     float pS1, pSA[MAXU], pB[3], pF[MAXG][3], pD[MAXD], pC[MAXC][3];
-    CSum S1, SA[MAXU], B[3], F[MAXG][3], D[MAXD], Cc[MAXC][3];
+    DSum S1, SA[MAXU], B[3], F[MAXG][3], D[MAXD], Cc[MAXC][3];
     float hh[MAXU], hl[MAXU];
-    int cnt;
     bool have;
 
     __device__ __forceinline__ void zero_partials()
@@ -160,7 +168,6 @@ struct Acc32 {
         for (int j = 0; j < MAXD; ++j) D[j].zero();
 #pragma unroll
         for (int j = 0; j < MAXC; ++j) { Cc[j][0].zero(); Cc[j][1].zero(); Cc[j][2].zero(); }
-        cnt = 0;
         have = false;
     }
 
@@ -184,7 +191,6 @@ struct Acc32 {
                 if (j < C.n_curl) { Cc[j][0].add(pC[j][0]); Cc[j][1].add(pC[j][1]); Cc[j][2].add(pC[j][2]); }
         }
         zero_partials();
-        cnt = 0;
     }
 };
 
@@ -264,7 +270,6 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_
             A.pC[0][2] += a[1] * gy - a[2] * gx;
         }
     }
-    if (++A.cnt == CHUNK) A.flush(C, need_grad);
 }
 
 __device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, const DevCatalog &C, int64_t qi)
@@ -394,9 +399,14 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         Acc32 A;
         setup32<STRAT>(T, sig, px, py, pz, bnear, Q, A, pay, stride);
         Slots S{0, -1};
+        int nb = 0;   // full batches since the last flush (warp-uniform)
         auto proc = [&](int fill) {
             if (!A.have) offsets_from(A, pay, stride, __shfl_sync(0xffffffffu, S.mine, 0));
             if (S.mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, S.mine);
+            if (fill == 32 && ++nb == CHUNK) {
+                A.flush(C, need_grad);
+                nb = 0;
+            }
         };
         if (T.root == 0) {
             double4 L;
@@ -439,7 +449,7 @@ __global__ void __launch_bounds__(128) k_pairs32w(DevTree T, DevCatalog C, const
         Query32 Q;
         Acc32 A;
         setup32<STRAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride);
-        int fill = 0;
+        int fill = 0, nb = 0;   // nb: full batches since the last flush (warp-uniform)
         int64_t mine = -1;
         for (int s0 = 0; s0 < ns; s0 += 32) {
             const int2 itm = s0 + lane < ns ? __ldg(P.items + j * ns + s0 + lane) : make_int2(-1, 0);
@@ -496,7 +506,11 @@ __global__ void __launch_bounds__(128) k_pairs32w(DevTree T, DevCatalog C, const
                             if (here) mine = (int64_t)lo + (tt - ex);
                         }
                         if (tb + 31 < tot) {
-                            if (mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);
+                            pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);   // full batch
+                            if (++nb == CHUNK) {
+                                A.flush(C, need_grad);
+                                nb = 0;
+                            }
                             mine = -1;
                             tb += 32;
                         } else {
