@@ -77,6 +77,9 @@ __device__ __forceinline__ void shape(float q, float &f, float &df)
     }
 }
 
+// support radius in units of h (the shapes vanish, with their derivatives, for q >= this)
+__host__ __device__ constexpr float ksupport(int k) { return k == 1 ? 2.5f : (k == 2 ? 3.f : 2.f); }
+
 __device__ __forceinline__ float ldexp_norm3(int k)
 {
     const float pi = 3.14159265358979f;
@@ -230,11 +233,20 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_
     float r = r2 * rinv;
     float W, G;
     if (STRAT == SYMMETRIC) {
-        float fa, dfa, fb, dfb;
+        float fa, dfa;
         shape<KT>(r * Q.ih, fa, dfa);
-        shape<KT>(r * p0.w, fb, dfb);
-        W = 0.5f * (Q.cw * fa + cWb * fb);
-        G = 0.5f * (Q.cg * dfa + cGb * dfb) * rinv;
+        // W(r, h_b) and its derivative are exactly zero outside the neighbour's own support;
+        // when that holds on every lane the h_b term is skipped (it would add exact zeros)
+        const float qb = r * p0.w;
+        float Wb = 0.f, Gb = 0.f;
+        if (__any_sync(__activemask(), qb < ksupport(KT))) {
+            float fb, dfb;
+            shape<KT>(qb, fb, dfb);
+            Wb = cWb * fb;
+            Gb = cGb * dfb;
+        }
+        W = 0.5f * (Q.cw * fa + Wb);
+        G = 0.5f * (Q.cg * dfa + Gb) * rinv;
     } else if (STRAT == GATHER) {
         float f, df;
         shape<KT>(r * Q.ih, f, df);
