@@ -274,6 +274,7 @@ def main():
     if world > 1:
         torch.distributed.barrier()
     launches = H.launch_count() - launches0
+    sched = H.schedule()
     clocks = sampler.stop()
     build_ms, interp_ms = float(np.mean(builds)), float(np.mean(interps))
     build_ms, interp_ms, step_ms = _max_over_ranks([build_ms, interp_ms, build_ms + interp_ms], world)
@@ -376,6 +377,7 @@ def main():
                 "build_ms": build_ms, "interp_ms": interp_ms,
                 "pts_per_s_with_build": world * npts / (step_ms / 1e3),
                 "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "schedule": dict(zip(("walk_rounds", "deferred_queries", "pool_chunks"), sched)),
                 "clocks": clocks, "accuracy_fp32c_vs_fp64": accuracy}
         txt = json.dumps(line)
         print(txt, flush=True)

@@ -25,6 +25,7 @@ namespace pb {
 __device__ const float g_line_inorm32[6][PB_LINE_NTAB] = PB_LINE_INORM_INIT;
 
 constexpr int CHUNK = 4;
+static_assert(CHUNK % 2 == 0, "pairs of batches must not straddle a flush");
 
 // ---- kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) in FP32 ----
 // Algebraically identical to the reference's piecewise forms but arranged so that nothing
@@ -37,43 +38,41 @@ template <int KT>
 __device__ __forceinline__ void shape(float q, float &f, float &df)
 {
     if (KT == 0) {   // M4
-        float a = fmaxf(2.f - q, 0.f);
-        float fi = 1.f + q * q * (0.75f * q - 1.5f), di = q * (2.25f * q - 3.f);
-        float fo = 0.25f * a * a * a, dO = -0.75f * a * a;
-        bool in = q < 1.f;
+        const float a = fmaxf(2.f - q, 0.f), a2 = a * a;
+        const float fi = fmaf(q * q, fmaf(0.75f, q, -1.5f), 1.f), di = q * fmaf(2.25f, q, -3.f);
+        const float fo = (0.25f * a2) * a, dO = -0.75f * a2;
+        const bool in = q < 1.f;
         f = in ? fi : fo;
         df = in ? di : dO;
     } else if (KT == 1) {   // M5
-        float a = fmaxf(2.5f - q, 0.f), b = fmaxf(1.5f - q, 0.f), c = fmaxf(0.5f - q, 0.f);
-        float a2 = a * a, b2 = b * b, c2 = c * c;
-        f = a2 * a2 - 5.f * b2 * b2 + 10.f * c2 * c2;
-        float q2 = q * q;
-        float di = q * (24.f * q2 - 30.f);
-        float dO = -4.f * a2 * a + 20.f * b2 * b;
+        const float a = fmaxf(2.5f - q, 0.f), b = fmaxf(1.5f - q, 0.f), c = fmaxf(0.5f - q, 0.f);
+        const float a2 = a * a, b2 = b * b, c2 = c * c;
+        f = fmaf(10.f * c2, c2, fmaf(-5.f * b2, b2, a2 * a2));
+        const float di = q * fmaf(24.f, q * q, -30.f);
+        const float dO = fmaf(20.f * b2, b, -4.f * a2 * a);
         df = q < 0.5f ? di : dO;
     } else if (KT == 2) {   // M6
-        float a = fmaxf(3.f - q, 0.f), b = fmaxf(2.f - q, 0.f), c = fmaxf(1.f - q, 0.f);
-        float a4 = (a * a) * (a * a), b4 = (b * b) * (b * b), c4 = (c * c) * (c * c);
-        f = a4 * a - 6.f * b4 * b + 15.f * c4 * c;
-        float q2 = q * q;
-        float di = q * (q2 * (120.f - 50.f * q) - 120.f);
-        float dO = -5.f * a4 + 30.f * b4;
+        const float a = fmaxf(3.f - q, 0.f), b = fmaxf(2.f - q, 0.f), c = fmaxf(1.f - q, 0.f);
+        const float a4 = (a * a) * (a * a), b4 = (b * b) * (b * b), c4 = (c * c) * (c * c);
+        f = fmaf(15.f * c4, c, fmaf(-6.f * b4, b, a4 * a));
+        const float di = q * fmaf(q * q, fmaf(-50.f, q, 120.f), -120.f);
+        const float dO = fmaf(30.f, b4, -5.f * a4);
         df = q < 1.f ? di : dO;
     } else if (KT == 3) {   // C2
-        float t = fmaxf(1.f - 0.5f * q, 0.f);
-        float t3 = t * t * t;
-        f = t3 * t * (2.f * q + 1.f);
-        df = -5.f * q * t3;
+        const float t = fmaxf(fmaf(-0.5f, q, 1.f), 0.f);
+        const float t3 = t * t * t;
+        f = (t3 * t) * fmaf(2.f, q, 1.f);
+        df = (-5.f * q) * t3;
     } else if (KT == 4) {   // C4
-        float t = fmaxf(1.f - 0.5f * q, 0.f);
-        float t5 = (t * t) * (t * t) * t;
-        f = t5 * t * ((35.f / 12.f) * q * q + 3.f * q + 1.f);
-        df = -(14.f / 3.f) * q * (1.f + 2.5f * q) * t5;
+        const float t = fmaxf(fmaf(-0.5f, q, 1.f), 0.f);
+        const float t5 = (t * t) * (t * t) * t;
+        f = (t5 * t) * fmaf(fmaf(35.f / 12.f, q, 3.f), q, 1.f);
+        df = ((-14.f / 3.f) * q) * fmaf(2.5f, q, 1.f) * t5;
     } else {   // C6
-        float t = fmaxf(1.f - 0.5f * q, 0.f);
-        float t7 = (t * t) * (t * t) * (t * t) * t;
-        f = t7 * t * (((4.f * q + 6.25f) * q + 4.f) * q + 1.f);
-        df = -5.5f * q * ((4.f * q + 3.5f) * q + 1.f) * t7;
+        const float t = fmaxf(fmaf(-0.5f, q, 1.f), 0.f);
+        const float t7 = (t * t) * (t * t) * (t * t) * t;
+        f = (t7 * t) * fmaf(fmaf(fmaf(4.f, q, 6.25f), q, 4.f), q, 1.f);
+        df = (-5.5f * q) * fmaf(fmaf(4.f, q, 3.5f), q, 1.f) * t7;
     }
 }
 
@@ -217,20 +216,25 @@ __device__ __forceinline__ void load_cols(const float4 *rec, int stride, float &
     for (int u = 0; u < MAXU; ++u) { ch[u] = v[2 + 2 * u]; cl[u] = v[3 + 2 * u]; }
 }
 
+// per-pair terms: weight m_b/rho_b W, quantity offsets a_u, weighted kernel gradient
+struct Terms32 {
+    float w, a[MAXU], gx, gy, gz;
+};
+
 template <int STRAT, int KT>
-__device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
-                                       const float4 *__restrict__ pay, int stride, int64_t b)
+__device__ __forceinline__ void terms32(const Acc32 &A, bool need_grad, const Query32 &Q,
+                                        const float4 *__restrict__ pay, int stride, int64_t b, Terms32 &t)
 {
     const float4 *rec = pay + b * stride;
-    float4 p0 = __ldg(rec), p1 = __ldg(rec + 1);
-    float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
-    float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
-    float dz = (Q.ph[2] - p0.z) + (Q.pl[2] - p1.z);
+    const float4 p0 = __ldg(rec), p1 = __ldg(rec + 1);
+    const float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
+    const float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
+    const float dz = (Q.ph[2] - p0.z) + (Q.pl[2] - p1.z);
     float cWb, cGb, ch[MAXU], cl[MAXU];
     load_cols(rec, stride, cWb, cGb, ch, cl);
-    float r2 = dx * dx + dy * dy + dz * dz;
-    float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
-    float r = r2 * rinv;
+    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+    const float r = r2 * rinv;
     float W, G;
     if (STRAT == SYMMETRIC) {
         float fa, dfa;
@@ -245,43 +249,73 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_
             Wb = cWb * fb;
             Gb = cGb * dfb;
         }
-        W = 0.5f * (Q.cw * fa + Wb);
-        G = 0.5f * (Q.cg * dfa + Gb) * rinv;
+        W = 0.5f * fmaf(Q.cw, fa, Wb);
+        G = (0.5f * fmaf(Q.cg, dfa, Gb)) * rinv;
     } else if (STRAT == GATHER) {
         float f, df;
         shape<KT>(r * Q.ih, f, df);
         W = Q.cw * f;
-        G = Q.cg * df * rinv;
+        G = (Q.cg * df) * rinv;
     } else {
         float f, df;
         shape<KT>(r * p0.w, f, df);
         W = cWb * f;
-        G = cGb * df * rinv;
+        G = (cGb * df) * rinv;
     }
     const float mrho = p1.w;
-    float w = mrho * W;
-    float a[MAXU];
+    t.w = mrho * W;
 #pragma unroll
-    for (int u = 0; u < MAXU; ++u) a[u] = (ch[u] - A.hh[u]) + (cl[u] - A.hl[u]);
-    A.pS1 += w;
-#pragma unroll
-    for (int u = 0; u < MAXU; ++u) A.pSA[u] += a[u] * w;
+    for (int u = 0; u < MAXU; ++u) t.a[u] = (ch[u] - A.hh[u]) + (cl[u] - A.hl[u]);
     if (need_grad) {
-        float gq = mrho * G;
-        float gx = gq * dx, gy = gq * dy, gz = gq * dz;
-        A.pB[0] += gx; A.pB[1] += gy; A.pB[2] += gz;
-        // fixed slots: the gradient's column in slot 0, the div/curl vector in slots 1..3
+        const float gq = mrho * G;
+        t.gx = gq * dx;
+        t.gy = gq * dy;
+        t.gz = gq * dz;
+    }
+}
+
+// fixed slots: the gradient's column in slot 0, the div/curl vector in slots 1..3
+__device__ __forceinline__ void accum32(Acc32 &A, const DevCatalog &C, bool need_grad, const Terms32 &t)
+{
+    A.pS1 += t.w;
+#pragma unroll
+    for (int u = 0; u < MAXU; ++u) A.pSA[u] = fmaf(t.a[u], t.w, A.pSA[u]);
+    if (need_grad) {
+        A.pB[0] += t.gx; A.pB[1] += t.gy; A.pB[2] += t.gz;
         if (C.n_grad > 0) {
-            const float av = a[0];
-            A.pF[0][0] += gx * av; A.pF[0][1] += gy * av; A.pF[0][2] += gz * av;
+            A.pF[0][0] = fmaf(t.gx, t.a[0], A.pF[0][0]);
+            A.pF[0][1] = fmaf(t.gy, t.a[0], A.pF[0][1]);
+            A.pF[0][2] = fmaf(t.gz, t.a[0], A.pF[0][2]);
         }
-        if (C.n_div > 0) A.pD[0] += gx * a[1] + gy * a[2] + gz * a[3];
+        if (C.n_div > 0) A.pD[0] = fmaf(t.gz, t.a[3], fmaf(t.gy, t.a[2], fmaf(t.gx, t.a[1], A.pD[0])));
         if (C.n_curl > 0) {
-            A.pC[0][0] += a[2] * gz - a[3] * gy;
-            A.pC[0][1] += a[3] * gx - a[1] * gz;
-            A.pC[0][2] += a[1] * gy - a[2] * gx;
+            A.pC[0][0] = fmaf(t.a[2], t.gz, fmaf(-t.a[3], t.gy, A.pC[0][0]));
+            A.pC[0][1] = fmaf(t.a[3], t.gx, fmaf(-t.a[1], t.gz, A.pC[0][1]));
+            A.pC[0][2] = fmaf(t.a[1], t.gy, fmaf(-t.a[2], t.gx, A.pC[0][2]));
         }
     }
+}
+
+template <int STRAT, int KT>
+__device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
+                                       const float4 *__restrict__ pay, int stride, int64_t b)
+{
+    Terms32 t;
+    terms32<STRAT, KT>(A, need_grad, Q, pay, stride, b, t);
+    accum32(A, C, need_grad, t);
+}
+
+// two pairs of one lane (consecutive in its sequence): independent terms, then accumulated
+// in order -- the same arithmetic as two pair32 calls, with twice the independent work
+template <int STRAT, int KT>
+__device__ __forceinline__ void pair32x2(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
+                                         const float4 *__restrict__ pay, int stride, int64_t b1, int64_t b2)
+{
+    Terms32 t1, t2;
+    terms32<STRAT, KT>(A, need_grad, Q, pay, stride, b1, t1);
+    terms32<STRAT, KT>(A, need_grad, Q, pay, stride, b2, t2);
+    accum32(A, C, need_grad, t1);
+    accum32(A, C, need_grad, t2);
 }
 
 __device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, const DevCatalog &C, int64_t qi)
@@ -441,7 +475,7 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
 // holding its leaf by a binary search over the inclusive prefix sums of the run lengths
 // held one per lane.
 template <int STRAT, int KT>
-__global__ void __launch_bounds__(128) k_pairs32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
+__global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
                                                   RunPool P, int64_t m, const uint32_t *__restrict__ ql,
                                                   const uint32_t *__restrict__ order, const double *__restrict__ qx,
                                                   const double *__restrict__ qy, const double *__restrict__ qz,
@@ -495,6 +529,23 @@ __global__ void __launch_bounds__(128) k_pairs32w(DevTree T, DevCatalog C, const
                         while (end0 <= t0 && r0 < 31) {
                             ++r0;
                             end0 = __shfl_sync(0xffffffffu, inc, r0);
+                        }
+                        if ((nb & 1) == 0 && tb >= 0 && tb + 64 <= (int64_t)end0) {
+                            // two full batches inside one run, flush boundary after the second
+                            if (rc != r0) {
+                                lo0 = __shfl_sync(0xffffffffu, rn.x, r0);
+                                ex0 = __shfl_sync(0xffffffffu, ex_own, r0);
+                                rc = r0;
+                            }
+                            const int64_t m1 = (int64_t)lo0 + ((unsigned)tb - ex0) + lane;
+                            pair32x2<STRAT, KT>(A, C, need_grad, Q, pay, stride, m1, m1 + 32);
+                            nb += 2;
+                            if (nb == CHUNK) {
+                                A.flush(C, need_grad);
+                                nb = 0;
+                            }
+                            tb += 64;
+                            continue;   // the next pass assigns or closes what is left of the chunk
                         }
                         if (tb >= 0 && tb + 32 <= (int64_t)end0) {
                             if (rc != r0) {
