@@ -304,7 +304,8 @@ def main():
             per[key] = {"kernel": name, "ms": float(ms), "algorithmic_bytes": alg[key], "achieved_gbs": a}
         dom = max(per, key=lambda k: per[k]["ms"])
         traffic = None
-        prof = os.path.join(REPO, "profiles", "%s_c2_traffic.json" % dom)
+        prof = os.path.join(REPO, "profiles", {"pairs": "k_pairs32w", "walk": "k_walk_items",
+                                                "fused": "k_points64w"}[dom] + "_c2_traffic.json")
         if os.path.exists(prof) and args.precision == "fp32c" and args.particles == (1 << 21) and \
                 args.grid == "256,256,64":
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")

@@ -22,8 +22,8 @@
  *     5 C6_Wendland; strategies: 0 itpGather, 1 itpScatter, 2 itpSymmetric
  *     (InterpolationStrategy.jl:1-5);
  *   - precision: PB_FP64 reproduces the reference's Float64 arithmetic in the reference's
- *     operation order; PB_FP32C runs the kernel sums in FP32 with compensated
- *     (TwoSum) accumulation and FP64 pair offsets, with the same neighbour sets.
+ *     operation order; PB_FP32C evaluates the per-pair kernel terms in FP32 (double-float
+ *     pair offsets) and accumulates FP32 chunk sums in FP64, with the same neighbour sets.
  */
 #ifndef PARTIA_B200_H
 #define PARTIA_B200_H
