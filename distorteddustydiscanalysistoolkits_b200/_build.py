@@ -27,6 +27,7 @@ UNITS = {
     "pb_interp64.cu": ["-fmad=false"],
     "pb_query.cu": ["-fmad=false"],
     "pb_walk.cu": ["-fmad=false"],
+    "pb_sched.cu": ["-fmad=false"],
     "pb_interp32.cu": ["-fmad=false"],   # FMAs only where written (fmaf): bits independent of code shape
     "pb_capi.cu": [],
     "pb_noalloc.cu": ["-fmad=false"],

@@ -61,7 +61,11 @@ EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set
             "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors", "pb_traversal_stats",
             "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
             "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc",
-            "pb_last_schedule"]
+            "pb_last_schedule", "pb_scheduler_features", "pb_scheduler_set", "pb_scheduler_get",
+            "pb_scheduler_predict", "pb_scheduler_gradients", "pb_scheduler_train"]
+
+SCHED_FEATURES = 16
+SCHED_PARAMS = 5313
 
 _lib = None
 
@@ -101,6 +105,13 @@ def load():
         "pb_launch_count": (ctypes.c_int64, [_vp]),
         "pb_last_timings": (ctypes.c_int32, [_vp, _dp, _dp, _lp]),
         "pb_last_schedule": (ctypes.c_int32, [_vp, _lp, _lp, _lp, _dp]),
+        "pb_scheduler_features": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp]),
+        "pb_scheduler_set": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_float, ctypes.c_int32]),
+        "pb_scheduler_get": (ctypes.c_int32, [_vp, _vp]),
+        "pb_scheduler_predict": (ctypes.c_int32, [_vp, _vp, ctypes.c_int64, _vp]),
+        "pb_scheduler_gradients": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp]),
+        "pb_scheduler_train": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.c_float, ctypes.c_uint64, _vp]),
         "pb_morton_sort_noalloc": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_int64, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():

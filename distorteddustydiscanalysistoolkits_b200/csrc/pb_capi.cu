@@ -27,7 +27,8 @@ pb::Handle::~Handle()
                    &right, &escape, &parent, &bmin64, &bmax64, &hmax64, &counters, &m_s, &rho_s, &col_ptrs,
                    &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux,
                    &pool_runs, &pool_next, &pool_ctr, &items, &wbnear, &qacc, &qflag, &cut, &defer_a, &defer_b,
-                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota};
+                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota, &mlp_w, &mlp_m, &mlp_v, &mlp_g, &mlp_norm,
+                   &mlp_scr, &mlp_idx, &mlp_x, &mlp_y, &mlp_loss, &sched_feat, &sched_pred, &sched_ql, &sched_tmp};
     for (DBuf *b : all) b->release();
     for (auto &b : in_cols) b.release();
     for (auto &b : cols_s) b.release();
@@ -498,82 +499,128 @@ int reserve_pool(Handle &H, int64_t m, int ns)
 }
 
 // FP32-compensated points in two phases: the walk kernels write every (query, subtree) item's
-// accepted runs, the pair kernel evaluates them (once per catalog launch, heaviest queries
-// first).  Queries that found the pool full are walked again in another round with an
-// emptied pool; if a round completes none of its queries, the fused walk-and-sum kernel takes
-// the rest.  Both kernels produce identical bits for a query.
+// accepted runs, the pair kernel evaluates them (once per catalog launch).  Queries go through
+// in slices of H.slice (Morton order when sorted), which bounds the item and pool memory.
+// Queries that found the pool full are walked again in another round with an emptied pool;
+// if a round completes fewer than 1/8 of its queries, the fused walk-and-sum kernel takes the
+// rest.  Both kernels produce identical bits for a query.
+//
+// Schedule modes (H.sched), all with identical results:
+//   0 plain:   queries in input order, one walk item per query, pairs in walk order;
+//   1 tuned:   Morton order, walk split into ~walk_split subtrees, pairs heaviest first;
+//   2 learned: as tuned, with the walk order binned by the MLP's predicted work
+//              (heaviest class first, Morton order inside a class).
 int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &launches, std::vector<double *> &dev,
                      int strategy, int64_t npts, const double *dx, const double *dy, const double *dz,
                      const uint32_t *perm)
 {
     if (npts > 0x7fffffffLL) return fail(H, PB_ERR_CAPACITY, "more than 2^31-1 sample points in one call");
+    const int mode = H.sched;
+    if (mode == 2 && !H.mlp_ready) return fail(H, PB_ERR_STATE, "learned schedule requested but no scheduler weights set");
     int ns = 1;
-    CK(launch_cut(&H, T, H.walk_split, &ns));
-    int rc = reserve_pool(H, npts, ns);
+    CK(launch_cut(&H, T, mode == 0 ? 1 : H.walk_split, &ns));
+    const int64_t S = H.slice > 0 ? std::min<int64_t>(H.slice, npts) : npts;
+    int rc = reserve_pool(H, S, ns);
     if (rc) return rc;
-    const uint32_t *ql = perm;
-    if (!ql) {
+    const uint32_t *ql_all = mode == 0 ? nullptr : perm;
+    if (!ql_all) {
         CK(H.iota.reserve(sizeof(uint32_t) * npts));
         CK(launch_iota(&H, npts, H.iota.as<uint32_t>()));
-        ql = H.iota.as<uint32_t>();
+        ql_all = H.iota.as<uint32_t>();
     }
-    int64_t m = npts;
+    if (mode == 2) {
+        CK(H.sched_feat.reserve(sizeof(float) * SCHED_F * S));
+        CK(H.sched_pred.reserve(sizeof(float) * S));
+        CK(H.sched_ql.reserve(sizeof(uint32_t) * S));
+        CK(H.sched_tmp.reserve(sizeof(uint32_t) * S));
+        CK(H.lpt_k.reserve(4 * S));
+        CK(H.lpt_v.reserve(4 * S));
+        CK(H.lpt_ka.reserve(4 * S));
+        CK(H.lpt_va.reserve(4 * S));
+    }
     uint32_t *lists[2] = {H.defer_a.as<uint32_t>(), H.defer_b.as<uint32_t>()};
     unsigned long long *ctr = H.pool_ctr.as<unsigned long long>();
     H.walk_rounds = 0;
     H.deferred_total = 0;
-    for (int round = 0;; ++round) {
-        CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
-        CK(cudaMemsetAsync(H.qacc.p, 0, sizeof(unsigned) * m, H.stream));
-        CK(cudaMemsetAsync(H.qflag.p, 0, sizeof(int) * m, H.stream));
-        RunPool P;
-        P.runs = H.pool_runs.as<uint2>();
-        P.next = H.pool_next.as<int>();
-        P.used = ctr;
-        P.cap = H.pool_cap;
-        P.ns = ns;
-        P.cut = H.cut.as<int2>() + (4 * H.walk_split + 8);
-        P.items = H.items.as<int2>();
-        P.bnear = H.wbnear.as<int>();
-        P.qacc = H.qacc.as<unsigned>();
-        P.qflag = H.qflag.as<int>();
-        P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
-        P.deferred = lists[round & 1];
-        if (round == 0) ev_record(H, 4);
-        if (strategy != SCATTER) {
-            CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
-            H.interp_launches++;
-        }
-        if (round == 0) ev_record(H, 5);
-        CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
-        H.interp_launches++;
-        uint32_t *order = nullptr;
-        CK(launch_lpt_order(&H, P, m, &order));
-        if (round == 0) ev_record(H, 6);
-        for (const Launch &Lc : launches) {
-            DevCatalog C = dev_catalog(H, Lc, dev.data());
-            CK(launch_pairs_fp32(&H, T, C, strategy, P, m, ql, order, dx, dy, dz));
-            H.interp_launches++;
-        }
-        if (round == 0) ev_record(H, 7);
-        unsigned nd = 0;
-        CK(cudaMemcpyAsync(&nd, P.n_deferred, sizeof(unsigned), cudaMemcpyDeviceToHost, H.stream));
-        CK(cudaStreamSynchronize(H.stream));
-        if (round == 0)
-            for (int k = 0; k < 3; ++k) H.t_phase_ms[k] = ev_ms(H, 4 + k, 5 + k);
-        H.walk_rounds = round + 1;
-        if (nd == 0) break;
-        H.deferred_total += nd;
-        if ((int64_t)nd > m - m / 8) {   // under 1/8 of the queries completed: finish them fused
-            for (const Launch &Lc : launches) {
-                DevCatalog C = dev_catalog(H, Lc, dev.data());
-                CK(launch_points_fp32(&H, T, C, strategy, nd, dx, dy, dz, P.deferred, npts));
+    for (int k = 0; k < 3; ++k) H.t_phase_ms[k] = 0.f;
+    for (int64_t s0 = 0; s0 < npts; s0 += S) {
+        const uint32_t *ql = ql_all + s0;
+        int64_t m = std::min<int64_t>(S, npts - s0);
+        for (int round = 0;; ++round) {
+            CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
+            CK(cudaMemsetAsync(H.qacc.p, 0, sizeof(unsigned) * m, H.stream));
+            CK(cudaMemsetAsync(H.qflag.p, 0, sizeof(int) * m, H.stream));
+            RunPool P;
+            P.runs = H.pool_runs.as<uint2>();
+            P.next = H.pool_next.as<int>();
+            P.used = ctr;
+            P.cap = H.pool_cap;
+            P.ns = ns;
+            P.cut = H.cut.as<int2>() + (4 * (mode == 0 ? 1 : H.walk_split) + 8);
+            P.items = H.items.as<int2>();
+            P.bnear = H.wbnear.as<int>();
+            P.qacc = H.qacc.as<unsigned>();
+            P.qflag = H.qflag.as<int>();
+            P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
+            P.deferred = lists[round & 1];
+            if (round == 0) ev_record(H, 4);
+            if (strategy != SCATTER || mode == 2) {
+                CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
                 H.interp_launches++;
             }
-            break;
+            if (mode == 2) {
+                // predicted work -> class-major walk order (Morton order kept inside a class)
+                float *feat = H.sched_feat.as<float>(), *pred = H.sched_pred.as<float>();
+                uint32_t *order = H.lpt_v.as<uint32_t>();
+                CK(launch_sched_features(&H, T, m, ql, dx, dy, dz, P.bnear, feat));
+                CK(launch_mlp_predict(&H, m, feat, pred));
+                CK(launch_sched_order(&H, m, pred, H.sched_width, H.sched_nclass, order));
+                uint32_t *qn = H.sched_ql.as<uint32_t>();
+                CK(launch_gather_u32(&H, m, order, ql, qn));
+                int *bt = reinterpret_cast<int *>(H.sched_tmp.as<uint32_t>());
+                CK(launch_gather_i32(&H, m, order, P.bnear, bt));
+                CK(cudaMemcpyAsync(P.bnear, bt, sizeof(int) * m, cudaMemcpyDeviceToDevice, H.stream));
+                ql = qn;
+                H.interp_launches += 4;
+            }
+            if (round == 0) ev_record(H, 5);
+            CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
+            H.interp_launches++;
+            uint32_t *order = nullptr;
+            if (mode != 0) CK(launch_lpt_order(&H, P, m, &order));
+            if (round == 0) ev_record(H, 6);
+            for (const Launch &Lc : launches) {
+                DevCatalog C = dev_catalog(H, Lc, dev.data());
+                CK(launch_pairs_fp32(&H, T, C, strategy, P, m, ql, order, dx, dy, dz));
+                H.interp_launches++;
+            }
+            if (round == 0) ev_record(H, 7);
+            unsigned nd = 0;
+            CK(cudaMemcpyAsync(&nd, P.n_deferred, sizeof(unsigned), cudaMemcpyDeviceToHost, H.stream));
+            CK(cudaStreamSynchronize(H.stream));
+            if (round == 0)
+                for (int k = 0; k < 3; ++k) H.t_phase_ms[k] += ev_ms(H, 4 + k, 5 + k);
+            H.walk_rounds = std::max<int64_t>(H.walk_rounds, round + 1);
+            if (nd == 0) break;
+            H.deferred_total += nd;
+            if ((int64_t)nd > m - m / 8) {   // under 1/8 of the queries completed: finish them fused
+                for (const Launch &Lc : launches) {
+                    DevCatalog C = dev_catalog(H, Lc, dev.data());
+                    CK(launch_points_fp32(&H, T, C, strategy, nd, dx, dy, dz, P.deferred, npts));
+                    H.interp_launches++;
+                }
+                break;
+            }
+            // the deferred list is walked next; in learned mode it is binned again
+            if (mode == 2) {
+                CK(cudaMemcpyAsync(H.sched_tmp.p, P.deferred, sizeof(uint32_t) * nd, cudaMemcpyDeviceToDevice,
+                                   H.stream));
+                ql = H.sched_tmp.as<uint32_t>();
+            } else {
+                ql = P.deferred;
+            }
+            m = nd;
         }
-        ql = P.deferred;
-        m = nd;
     }
     return PB_OK;
 }
@@ -738,7 +785,13 @@ int32_t pb_set_option(pb_handle *h, const char *name, int64_t value)
     if (!strcmp(name, "timing")) H.timing = value != 0;
     else if (!strcmp(name, "sort_queries")) H.sort_queries = (int)value;
     else if (!strcmp(name, "block_size")) H.block_size = (int)value;
-    else if (!strcmp(name, "walk_split")) {
+    else if (!strcmp(name, "schedule")) {
+        if (value < 0 || value > 2) return fail(H, PB_ERR_INVALID, "schedule must be 0 (plain), 1 (tuned) or 2 (learned)");
+        H.sched = (int)value;
+    } else if (!strcmp(name, "slice_queries")) {
+        if (value < 1024) return fail(H, PB_ERR_INVALID, "slice_queries must be >= 1024");
+        H.slice = value;
+    } else if (!strcmp(name, "walk_split")) {
         if (value < 1 || value > 4096) return fail(H, PB_ERR_INVALID, "walk_split must be in 1..4096");
         H.walk_split = (int)value;
     }
@@ -945,6 +998,160 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
 }
 
 int64_t pb_launch_count(const pb_handle *h) { return h ? h->H.launches : 0; }
+
+// ---- learned work prediction ----
+namespace {
+// device view of a float array given as host or device memory (staged into `buf`)
+int stage_f32(Handle &H, DBuf &buf, const float *src, int64_t n, const float **out)
+{
+    if (is_device_ptr(src)) {
+        *out = src;
+        return PB_OK;
+    }
+    CK(buf.reserve(sizeof(float) * (n > 0 ? n : 1)));
+    CK(cudaMemcpyAsync(buf.p, src, sizeof(float) * n, cudaMemcpyHostToDevice, H.stream));
+    *out = buf.as<float>();
+    return PB_OK;
+}
+
+int copy_out_f32(Handle &H, float *dst, const float *src, int64_t n)
+{
+    CK(cudaMemcpyAsync(dst, src, sizeof(float) * n, cudaMemcpyDefault, H.stream));
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
+
+int mlp_reserve(Handle &H)
+{
+    CK(H.mlp_w.reserve(sizeof(float) * SCHED_NPARAM));
+    CK(H.mlp_m.reserve(sizeof(float) * SCHED_NPARAM));
+    CK(H.mlp_v.reserve(sizeof(float) * SCHED_NPARAM));
+    CK(H.mlp_g.reserve(sizeof(float) * SCHED_NPARAM));
+    CK(H.mlp_norm.reserve(sizeof(float) * 2 * SCHED_F));
+    return PB_OK;
+}
+}  // namespace
+
+int32_t pb_scheduler_features(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                              float *feat)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (npts < 0 || !feat) return fail(H, PB_ERR_INVALID, "bad arguments");
+    if (npts == 0) return PB_OK;
+    CK(cudaSetDevice(H.device));
+    const double *dx, *dy, *dz;
+    int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
+    if (rc) return rc;
+    float *out = feat;
+    if (!is_device_ptr(feat)) {
+        CK(H.sched_feat.reserve(sizeof(float) * SCHED_F * npts));
+        out = H.sched_feat.as<float>();
+    }
+    DevTree T = make_tree(H);
+    CK(launch_sched_features(&H, T, npts, nullptr, dx, dy, dz, nullptr, out));
+    if (out != feat) return copy_out_f32(H, feat, out, SCHED_F * npts);
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
+
+int32_t pb_scheduler_set(pb_handle *h, const float *params, const float *norm, float bin_width, int32_t nclass)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!params || !norm || !(bin_width > 0.f) || nclass < 1 || nclass > 1024)
+        return fail(H, PB_ERR_INVALID, "scheduler weights: bad arguments");
+    CK(cudaSetDevice(H.device));
+    int rc = mlp_reserve(H);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(H.mlp_w.p, params, sizeof(float) * SCHED_NPARAM, cudaMemcpyDefault, H.stream));
+    CK(cudaMemcpyAsync(H.mlp_norm.p, norm, sizeof(float) * 2 * SCHED_F, cudaMemcpyDefault, H.stream));
+    CK(cudaStreamSynchronize(H.stream));
+    H.sched_width = bin_width;
+    H.sched_nclass = nclass;
+    H.mlp_ready = true;
+    return PB_OK;
+}
+
+int32_t pb_scheduler_get(pb_handle *h, float *params)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.mlp_ready) return fail(H, PB_ERR_STATE, "no scheduler weights set");
+    CK(cudaSetDevice(H.device));
+    return copy_out_f32(H, params, H.mlp_w.as<float>(), SCHED_NPARAM);
+}
+
+int32_t pb_scheduler_predict(pb_handle *h, const float *X, int64_t n, float *out)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.mlp_ready) return fail(H, PB_ERR_STATE, "no scheduler weights set");
+    if (n < 0 || !X || !out) return fail(H, PB_ERR_INVALID, "bad arguments");
+    if (n == 0) return PB_OK;
+    CK(cudaSetDevice(H.device));
+    const float *dX;
+    int rc = stage_f32(H, H.mlp_x, X, n * SCHED_F, &dX);
+    if (rc) return rc;
+    CK(H.sched_pred.reserve(sizeof(float) * n));
+    CK(launch_mlp_predict(&H, n, dX, H.sched_pred.as<float>()));
+    return copy_out_f32(H, out, H.sched_pred.as<float>(), n);
+}
+
+int32_t pb_scheduler_gradients(pb_handle *h, const float *X, const float *y, int64_t n, float *grads, float *loss)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.mlp_ready) return fail(H, PB_ERR_STATE, "no scheduler weights set");
+    if (n < 1 || !X || !y || !grads) return fail(H, PB_ERR_INVALID, "bad arguments");
+    CK(cudaSetDevice(H.device));
+    const float *dX, *dy;
+    int rc = stage_f32(H, H.mlp_x, X, n * SCHED_F, &dX);
+    if (!rc) rc = stage_f32(H, H.mlp_y, y, n, &dy);
+    if (rc) return rc;
+    CK(launch_mlp_grad(&H, n, dX, dy, nullptr, nullptr));
+    if ((rc = copy_out_f32(H, grads, H.mlp_g.as<float>(), SCHED_NPARAM))) return rc;
+    if (loss) {
+        std::vector<float> sq(n);
+        if ((rc = copy_out_f32(H, sq.data(), mlp_last_sq(&H, n), n))) return rc;
+        double acc = 0.0;
+        for (float v : sq) acc += v;
+        *loss = (float)(acc / (double)n);
+    }
+    return PB_OK;
+}
+
+int32_t pb_scheduler_train(pb_handle *h, const float *X, const float *y, int64_t n, int32_t steps, int32_t batch,
+                           float lr, uint64_t seed, float *losses)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.mlp_ready) return fail(H, PB_ERR_STATE, "set initial scheduler weights first (pb_scheduler_set)");
+    if (n < 1 || !X || !y || steps < 0 || batch < 1) return fail(H, PB_ERR_INVALID, "bad arguments");
+    CK(cudaSetDevice(H.device));
+    const float *dX, *dy;
+    int rc = stage_f32(H, H.mlp_x, X, n * SCHED_F, &dX);
+    if (!rc) rc = stage_f32(H, H.mlp_y, y, n, &dy);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(H.mlp_m.p, 0, sizeof(float) * SCHED_NPARAM, H.stream));
+    CK(cudaMemsetAsync(H.mlp_v.p, 0, sizeof(float) * SCHED_NPARAM, H.stream));
+    CK(H.mlp_idx.reserve(sizeof(int64_t) * batch));
+    std::vector<float> sq(losses ? batch : 0);
+    for (int32_t t = 0; t < steps; ++t) {
+        CK(launch_draw(&H, batch, n, seed, (unsigned long long)t, H.mlp_idx.as<int64_t>()));
+        CK(launch_mlp_grad(&H, batch, dX, dy, H.mlp_idx.as<int64_t>(), nullptr));
+        CK(launch_mlp_adam(&H, lr, t + 1));
+        if (losses) {
+            if ((rc = copy_out_f32(H, sq.data(), mlp_last_sq(&H, batch), batch))) return rc;
+            double acc = 0.0;
+            for (float v : sq) acc += v;
+            losses[t] = (float)(acc / (double)batch);
+        }
+    }
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
 
 int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks,
                          double *phase_ms)

@@ -33,6 +33,11 @@ struct DBuf {
     template <typename T> T *as() const { return static_cast<T *>(p); }
 };
 
+// learned schedule: MLP of SCHED_F features -> SCHED_H -> SCHED_H -> 1
+constexpr int SCHED_F = 16;
+constexpr int SCHED_H = 64;
+constexpr int SCHED_NPARAM = SCHED_H * SCHED_F + SCHED_H + SCHED_H * SCHED_H + SCHED_H + SCHED_H + 1;
+
 struct QuantParams {
     double vmin[3];
     double inv[3];
@@ -70,6 +75,14 @@ struct Handle {
     DBuf pool_runs, pool_next, pool_ctr, items, wbnear, qacc, qflag, cut, defer_a, defer_b, lpt_k, lpt_v, lpt_ka,
         lpt_va, iota;
     int walk_split = 64;   // target number of subtrees each query's walk is split into
+    int sched = 1;         // 0 plain (input order, one walk per query, no ordering), 1 tuned, 2 learned
+    int64_t slice = int64_t(1) << 22;   // queries per two-phase slice
+    // learned work prediction (pb_sched.cu)
+    DBuf mlp_w, mlp_m, mlp_v, mlp_g, mlp_norm, mlp_scr, mlp_idx, mlp_x, mlp_y, mlp_loss, sched_feat, sched_pred,
+        sched_ql, sched_tmp;
+    bool mlp_ready = false;
+    float sched_width = 1.f;
+    int sched_nclass = 16;
     unsigned long long pool_cap = 0;
     int64_t walk_rounds = 0, deferred_total = 0;
 
@@ -112,6 +125,19 @@ cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool
                         const double *qx, const double *qy, const double *qz, unsigned long long *counter);
 cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order);
 cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out);
+
+// ---- launchers (pb_sched.cu) ----
+cudaError_t launch_sched_features(Handle *H, const DevTree &T, int64_t m, const uint32_t *ql, const double *qx,
+                                  const double *qy, const double *qz, const int *bnear, float *feat);
+cudaError_t launch_mlp_predict(Handle *H, int64_t n, const float *X, float *y);
+cudaError_t launch_mlp_grad(Handle *H, int64_t nb, const float *X, const float *T, const int64_t *idx, float *loss);
+const float *mlp_last_sq(Handle *H, int64_t nb);
+cudaError_t launch_mlp_adam(Handle *H, float lr, int64_t step);
+cudaError_t launch_draw(Handle *H, int64_t nb, int64_t n, unsigned long long seed, unsigned long long step,
+                        int64_t *idx);
+cudaError_t launch_sched_order(Handle *H, int64_t m, const float *pred, float width, int nclass, uint32_t *order);
+cudaError_t launch_gather_u32(Handle *H, int64_t m, const uint32_t *order, const uint32_t *src, uint32_t *dst);
+cudaError_t launch_gather_i32(Handle *H, int64_t m, const uint32_t *order, const int *src, int *dst);
 
 // ---- launchers (pb_interp64.cu / pb_interp32.cu / pb_query.cu) ----
 cudaError_t launch_pairs_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, const RunPool &P,

@@ -55,6 +55,70 @@ def dusty_disc(n_gas, n_dust, seed=3, tilt_deg=30.0, dust_to_gas=0.01):
     return gas, dust
 
 
+def clumped_disc(n, seed=5, mass=None, tilt_deg=30.0, n_clumps=2000, clump_fraction=0.1, pitch_deg=12.0,
+                 arm_contrast=5.0, arm_width=0.1, rmin=1.0, rmax=100.0):
+    """Disc with two logarithmic spiral arms and Gaussian clumps (about 100x spread in h).
+
+    The base disc is ``disc``'s (Sigma ~ 1/r, H = 0.05 r^1.25, warp ramping to ``tilt_deg``);
+    its azimuths follow two log spirals phi_arm = phi0 + ln(r) / tan(pitch) (+ pi) with a
+    Gaussian profile of width ``arm_width`` rad and an arm/inter-arm density contrast
+    ``arm_contrast``.  ``n_clumps`` Gaussian clumps (centres drawn from the disc, sigma
+    log-uniform in [0.05, 0.5] H(r)) share ``clump_fraction`` of the particles equally.  Every
+    particle has the same mass (total 1 unless given); h = 1.2 (m/rho)^(1/3) from the analytic
+    density of its own component."""
+    g = _rng(seed)
+    m = (1.0 / n) if mass is None else mass
+    n_cl_each = int(n * clump_fraction) // n_clumps
+    n_cl = n_cl_each * n_clumps
+    nd = n - n_cl
+    r = g.uniform(rmin, rmax, nd)
+    # azimuths by rejection against the arm profile w(phi) = 1 + (c - 1) exp(-dphi^2 / 2 w^2)
+    k = 1.0 / math.tan(math.radians(pitch_deg))
+    phi0 = g.uniform(0.0, 2.0 * np.pi)
+    phi = np.empty(nd)
+    todo = np.arange(nd)
+    while len(todo):
+        cand = g.uniform(0.0, 2.0 * np.pi, len(todo))
+        d = np.mod(cand - (phi0 + k * np.log(r[todo])), np.pi)
+        d = np.minimum(d, np.pi - d)
+        w = 1.0 + (arm_contrast - 1.0) * np.exp(-d * d / (2.0 * arm_width ** 2))
+        ok = g.uniform(0.0, arm_contrast, len(todo)) < w
+        phi[todo[ok]] = cand[ok]
+        todo = todo[~ok]
+    d = np.mod(phi - (phi0 + k * np.log(r)), np.pi)
+    d = np.minimum(d, np.pi - d)
+    w = 1.0 + (arm_contrast - 1.0) * np.exp(-d * d / (2.0 * arm_width ** 2))
+    wmean = 1.0 + (arm_contrast - 1.0) * arm_width * math.sqrt(2.0 * math.pi) / np.pi
+    H = 0.05 * r ** 1.25
+    zp = g.normal(0.0, 1.0, nd) * H
+    sigma = nd * m / (2.0 * np.pi * (rmax - rmin) * r)
+    rho = sigma / (math.sqrt(2.0 * np.pi) * H) * np.exp(-zp * zp / (2.0 * H * H)) * w / wmean
+    # clumps: centres drawn from the disc particles, isotropic Gaussians
+    ci = g.integers(0, nd, n_clumps)
+    cr, cphi, cz = r[ci], phi[ci], zp[ci]
+    csig = np.exp(g.uniform(math.log(0.05), math.log(0.5), n_clumps)) * (0.05 * cr ** 1.25)
+    off = g.normal(0.0, 1.0, (3, n_cl)) * np.repeat(csig, n_cl_each)
+    cx0 = np.repeat(cr * np.cos(cphi), n_cl_each) + off[0]
+    cy0 = np.repeat(cr * np.sin(cphi), n_cl_each) + off[1]
+    cz0 = np.repeat(cz, n_cl_each) + off[2]
+    q2 = (off ** 2).sum(0) / np.repeat(csig, n_cl_each) ** 2
+    rho_c = n_cl_each * m / ((2.0 * np.pi) ** 1.5 * np.repeat(csig, n_cl_each) ** 3) * np.exp(-0.5 * q2)
+    x0 = np.concatenate([r * np.cos(phi), cx0])
+    y0 = np.concatenate([r * np.sin(phi), cy0])
+    z0 = np.concatenate([zp, cz0])
+    rho = np.concatenate([rho, rho_c])
+    rr = np.sqrt(x0 * x0 + y0 * y0)
+    h = 1.2 * (m / rho) ** (1.0 / 3.0)
+    beta = np.deg2rad(tilt_deg) * (np.clip(rr, rmin, rmax) - rmin) / (rmax - rmin)
+    cb, sb = np.cos(beta), np.sin(beta)
+    vk = np.maximum(rr, rmin) ** -0.5
+    ph = np.arctan2(y0, x0)
+    vx0, vy0 = -vk * np.sin(ph), vk * np.cos(ph)
+    noise = g.normal(0.0, 1.0, (3, n)) * (0.01 * vk)
+    return {"x": x0, "y": y0 * cb - z0 * sb, "z": y0 * sb + z0 * cb, "m": np.full(n, m), "h": h, "rho": rho,
+            "vx": vx0 + noise[0], "vy": vy0 * cb + noise[1], "vz": vy0 * sb + noise[2]}
+
+
 def cartesian_box_grid(p, n=64, pad=0.0):
     """Cartesian n^3 grid spanning the particle bounding box."""
     lo = [float(np.min(p[k])) - pad for k in "xyz"]

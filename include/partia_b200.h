@@ -80,7 +80,11 @@ int32_t pb_last_error(const pb_handle *h, char *buf, int64_t size);
 int32_t pb_set_stream(pb_handle *h, void *cuda_stream);
 /* Options: "timing" (record CUDA events around build/traversal), "sort_queries"
    (Morton-order queries before traversal; schedule only), "block_size", "walk_split" (target
-   number of subtrees each FP32-compensated point walk is split into, 1..4096; schedule only). */
+   number of subtrees each FP32-compensated point walk is split into, 1..4096; schedule only),
+   "schedule" (FP32-compensated points: 0 plain = input order, one walk per query, no
+   ordering; 1 tuned = Morton order, split walks, heaviest first (default); 2 learned = tuned
+   plus binning by predicted work; results are identical), "slice_queries" (queries per
+   walk/sum slice, default 2^22). */
 int32_t pb_set_option(pb_handle *h, const char *name, int64_t value);
 
 /* LinearBVH!(input, Val(3)) (InterpolationInput.jl:203-223): MortonEncoding
@@ -167,6 +171,29 @@ int32_t pb_morton_sort_noalloc(const double *x, const double *y, const double *z
    the last call in ms (needs option "timing"); traversal kernel launches of the last call. */
 int64_t pb_launch_count(const pb_handle *h);
 int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms, int64_t *interp_launches);
+
+/* Learned work prediction for the FP32-compensated point schedule (no counterpart in the
+   reference; the reference runs queries in input order).  A 3-layer MLP of width 64 with
+   BF16 weights and activations (PB_SCHED_FEATURES inputs, PB_SCHED_PARAMS parameters laid out
+   W1[64][F], b1[64], W2[64][64], b2[64], W3[64], b3) predicts log2(1 + accepted neighbours) of
+   a sample point; option "schedule" = 2 then walks the queries binned by predicted work
+   (class = floor(prediction / bin_width), heaviest first).  Outputs do not depend on it.
+   pb_scheduler_features: the npts x F features of sample points on the last build.
+   pb_scheduler_set: weights, input normalisation norm[2F] = (mean[F], 1/std[F]), bins.
+   pb_scheduler_train: Adam on the device (own forward/backward kernels), minibatches drawn
+   with `seed`, starting from the current weights; losses[steps] (may be NULL) = batch MSE.
+   pb_scheduler_gradients: gradient of the mean squared error over all n samples.
+   Arrays may be host or device memory. */
+#define PB_SCHED_FEATURES 16
+#define PB_SCHED_PARAMS 5313
+int32_t pb_scheduler_features(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                              float *feat);
+int32_t pb_scheduler_set(pb_handle *h, const float *params, const float *norm, float bin_width, int32_t nclass);
+int32_t pb_scheduler_get(pb_handle *h, float *params);
+int32_t pb_scheduler_predict(pb_handle *h, const float *X, int64_t n, float *out);
+int32_t pb_scheduler_gradients(pb_handle *h, const float *X, const float *y, int64_t n, float *grads, float *loss);
+int32_t pb_scheduler_train(pb_handle *h, const float *X, const float *y, int64_t n, int32_t steps, int32_t batch,
+                           float lr, uint64_t seed, float *losses);
 
 /* Diagnostics of the last FP32-compensated point call (no counterpart in the reference):
    walk rounds taken, queries deferred because the accepted-run pool was full (they are walked
