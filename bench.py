@@ -49,8 +49,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
-    ap.add_argument("--particles", type=int, default=1 << 21)
-    ap.add_argument("--grid", default="256,256,64")
+    ap.add_argument("--config", default="c2", choices=["c2", "c5"],
+                    help="c2: warped disc, cylindrical grid, L=11 (the headline); c5: clumped 16M disc, "
+                         "C4 Wendland, rho + curl v on a 256^3 Cartesian grid")
+    ap.add_argument("--schedule", default="learned", choices=["plain", "tuned", "learned"],
+                    help="query schedule of the FP32C path (outputs are identical)")
+    ap.add_argument("--no-schedules", action="store_true", help="skip the plain/tuned/learned comparison")
+    ap.add_argument("--particles", type=int, default=None)
+    ap.add_argument("--grid", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -63,17 +69,30 @@ def parse():
 def workload(args, rank):
     from distorteddustydiscanalysistoolkits_b200 import synthetic
     import distorteddustydiscanalysistoolkits_b200 as pb
-    ns, nphi, nz = (int(v) for v in args.grid.split(","))
-    p = synthetic.disc(args.particles, seed=2 + rank)
+    if args.config == "c5":
+        n = args.particles or (1 << 24)
+        g = int(args.grid or 256)
+        p = synthetic.clumped_disc(n, seed=5 + rank)
+        flat = pb.flatten(pb.Cartesian, synthetic.cartesian_box_grid(p, n=g))
+        cols = synthetic.C2_COLUMNS
+        cat = pb.InterpolationCatalog(cols, scalars=("rho",), curls=("v",))
+        config = {"workload": "clumped disc (two log spirals + 2000 clumps), %d particles (C4 Wendland), "
+                              "Cartesian %d^3 grid, itpSymmetric, L=%d (rho; curl v)" % (n, g, cat.L),
+                  "particles": n, "grid_points": len(flat), "outputs": cat.L, "kernel": "C4_Wendland",
+                  "strategy": "itpSymmetric", "precision": args.precision}
+        return p, flat, cols, cat, config, pb.C4_Wendland
+    n = args.particles or (1 << 21)
+    ns, nphi, nz = (int(v) for v in (args.grid or "256,256,64").split(","))
+    p = synthetic.disc(n, seed=2 + rank)
     grid = synthetic.log_cylindrical_grid(ns, nphi, nz)
     flat = pb.flatten(pb.Cylindrical, grid)
     cols = synthetic.C2_COLUMNS
     cat = pb.InterpolationCatalog(cols, **synthetic.C2_CATALOG)
     config = {"workload": "warped gas disc, %d particles (M4), cylindrical %dx%dx%d log-r grid, itpSymmetric, "
-                          "L=%d (rho,vx,vy,vz; grad rho; div v; curl v)" % (args.particles, ns, nphi, nz, cat.L),
-              "particles": args.particles, "grid_points": len(flat), "outputs": cat.L, "kernel": "M4_spline",
+                          "L=%d (rho,vx,vy,vz; grad rho; div v; curl v)" % (n, ns, nphi, nz, cat.L),
+              "particles": n, "grid_points": len(flat), "outputs": cat.L, "kernel": "M4_spline",
               "strategy": "itpSymmetric", "precision": args.precision}
-    return p, flat, cols, cat, config
+    return p, flat, cols, cat, config, pb.M4_spline
 
 
 def _max_over_ranks(vals, world):
@@ -176,7 +195,7 @@ def run_reference(args, rank, world):
         return 0
     import oracle
     import distorteddustydiscanalysistoolkits_b200 as pb  # noqa: F401  (catalog/grid host types only)
-    p, flat, cols, cat, config = workload(args, 0)
+    p, flat, cols, cat, config, _ = workload(args, 0)
     threads = oracle.max_threads()
     t0 = time.perf_counter()
     o = oracle.OracleLBVH(p["x"], p["y"], p["z"], p["h"]).attach(p["m"], p["rho"], [p[c] for c in cols])
@@ -228,12 +247,21 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    p, flat, cols, cat, config = workload(args, rank)
+    p, flat, cols, cat, config, skern = workload(args, rank)
+    nparticles = len(p["x"])
     prec = pb.FP32C if args.precision == "fp32c" else pb.FP64
     npts = len(flat)
     backend = pb.CUDAComputeBackend(local)
     H = backend.handle
     H.set_option("timing", 1)
+    from distorteddustydiscanalysistoolkits_b200 import scheduler
+    sched_modes = {"plain": scheduler.PLAIN, "tuned": scheduler.TUNED, "learned": scheduler.LEARNED}
+    model = scheduler.Model.load() if os.path.exists(scheduler.MODEL_PATH) else None
+    if model is not None:
+        scheduler.set_model(H, model)
+    if args.schedule == "learned" and model is None:
+        args.schedule = "tuned"
+    H.set_option("schedule", sched_modes[args.schedule])
     stream = torch.cuda.current_stream()
     H.set_stream(stream.cuda_stream)
 
@@ -241,7 +269,7 @@ def main():
     q = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in flat.coor]
     outs = [torch.empty(npts, dtype=torch.float64, device="cuda") for _ in range(cat.L)]
     inp = pb.InterpolationInput(dev["x"], dev["y"], dev["z"], dev["m"], dev["h"], dev["rho"],
-                                tuple(dev[c] for c in cols), smoothed_kernel=pb.M4_spline)
+                                tuple(dev[c] for c in cols), smoothed_kernel=skern)
     import ctypes
     cin, ccat = inp._c_struct(), cat._c_struct()
     optrs = (ctypes.c_void_p * cat.L)(*[o.data_ptr() for o in outs])
@@ -280,14 +308,41 @@ def main():
         torch.distributed.barrier()
     launches = H.launch_count() - launches0
     sched = H.schedule()
+    main_phases = list(phases)
     clocks = sampler.stop()
     build_ms, interp_ms = float(np.mean(builds)), float(np.mean(interps))
     build_ms, interp_ms, step_ms = _max_over_ranks([build_ms, interp_ms, build_ms + interp_ms], world)
     value = world * npts / (interp_ms / 1e3)
 
+    # the same step under each query schedule (identical outputs): plain = input order, one walk
+    # per query, no ordering; tuned = Morton order, split walks, heaviest-first pairs; learned =
+    # tuned + walk order binned by the MLP's predicted work
+    schedules = None
+    if prec == pb.FP32C and not args.no_schedules:
+        schedules = {}
+        for name, mode in sched_modes.items():
+            if mode == scheduler.LEARNED and model is None:
+                continue
+            H.set_option("schedule", mode)
+            for _ in range(2):
+                step()
+            phases.clear()
+            ts = []
+            for _ in range(max(2, min(args.steps, 3))):
+                flush.zero_()
+                ts.append(step()[1])
+            ph = np.mean(np.array(phases), axis=0)
+            schedules[name] = {"interp_ms": float(np.mean(ts)), "pts_per_s": npts / (float(np.mean(ts)) / 1e3),
+                               "nearest_ms": float(ph[0]), "walk_ms": float(ph[1]), "pairs_ms": float(ph[2])}
+        H.set_option("schedule", sched_modes[args.schedule])
+        if "plain" in schedules:
+            for name in schedules:
+                schedules[name]["speedup_vs_plain"] = schedules["plain"]["interp_ms"] / schedules[name]["interp_ms"]
+        phases.clear()
+
     # roofline of the dominant kernel phase (FP32C: walk kernels vs pair kernel, per-phase CUDA
     # events of the library; FP64: the fused kernel)
-    lb = pb.LinearBVH(backend, args.particles)
+    lb = pb.LinearBVH(backend, nparticles)
     roofline = None
     if not args.no_roofline:
         stats = pb.traversal_stats(lb, [c.cpu().numpy() for c in q], pb.itpSymmetric)
@@ -296,10 +351,11 @@ def main():
         peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(REPO, "MEASURED_PEAKS.json")) else None
         peak = peaks["hbm_gbs"] if peaks else 6650.0
-        ph = np.mean(np.array(phases), axis=0) if phases else np.zeros(3)
+        ph = np.mean(np.array(main_phases), axis=0) if main_phases else np.zeros(3)
         if prec == pb.FP32C:
+            kname = {"M4_spline": "M4", "C4_Wendland": "C4"}.get(config["kernel"], config["kernel"])
             kern = {"walk": ("k_nearest_list + k_walk_items<itpSymmetric>", ph[0] + ph[1]),
-                    "pairs": ("k_pairs32w<itpSymmetric,M4>", ph[2])}
+                    "pairs": ("k_pairs32w<itpSymmetric,%s>" % kname, ph[2])}
         else:
             kern = {"fused": ("k_points64w<itpSymmetric>", interp_ms)}
             alg = {"fused": alg["walk"] + alg["pairs"]}
@@ -311,8 +367,8 @@ def main():
         traffic = None
         prof = os.path.join(REPO, "profiles", {"pairs": "k_pairs32w", "walk": "k_walk_items",
                                                 "fused": "k_points64w"}[dom] + "_c2_traffic.json")
-        if os.path.exists(prof) and args.precision == "fp32c" and args.particles == (1 << 21) and \
-                args.grid == "256,256,64":
+        if os.path.exists(prof) and args.precision == "fp32c" and args.config == "c2" and \
+                args.particles in (None, 1 << 21) and args.grid in (None, "256,256,64"):
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")
         achieved = per[dom]["achieved_gbs"]
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -355,7 +411,7 @@ def main():
             for key in hp:
                 hp[key][:] = pristine[key]
             inp_h = pb.InterpolationInput(hp["x"], hp["y"], hp["z"], hp["m"], hp["h"], hp["rho"],
-                                          tuple(hp[c] for c in cols), smoothed_kernel=pb.M4_spline)
+                                          tuple(hp[c] for c in cols), smoothed_kernel=skern)
             t0 = time.perf_counter()
             pb.PointSamples_interpolation(backend, grid, inp_h, cat, pb.itpSymmetric, precision=prec, out=hout)
             dt = time.perf_counter() - t0
@@ -364,8 +420,8 @@ def main():
         e2e_s = _max_over_ranks([float(np.mean(times))], world)[0]
         ncols_in = 6 + len(cols)
         e2e = {"value": world * npts / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3,
-               "h2d_bytes_per_step": ncols_in * 8 * args.particles + 24 * npts,
-               "d2h_bytes_per_step": cat.L * 8 * npts + ncols_in * 8 * args.particles,
+               "h2d_bytes_per_step": ncols_in * 8 * nparticles + 24 * npts,
+               "d2h_bytes_per_step": cat.L * 8 * npts + ncols_in * 8 * nparticles,
                "path": "PointSamples_interpolation(CUDAComputeBackend) with pinned host arrays: H2D, build, "
                        "interpolation, D2H of outputs and of the permuted particle columns"}
 
@@ -383,7 +439,8 @@ def main():
                 "build_ms": build_ms, "interp_ms": interp_ms,
                 "pts_per_s_with_build": world * npts / (step_ms / 1e3),
                 "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "schedule": dict(zip(("walk_rounds", "deferred_queries", "pool_chunks"), sched)),
+                "schedule": dict(zip(("walk_rounds", "deferred_queries", "pool_chunks"), sched), mode=args.schedule),
+                "schedules": schedules,
                 "clocks": clocks, "accuracy_fp32c_vs_fp64": accuracy}
         txt = json.dumps(line)
         print(txt, flush=True)

@@ -498,6 +498,50 @@ int reserve_pool(Handle &H, int64_t m, int ns)
     return PB_OK;
 }
 
+// Fused walk-and-sum for the queries a full pool left over (P.deferred[0..nd)).  Their exact
+// accepted counts come from a counting walk, so the light ones get the FP64 kernel and the
+// heavy ones the FP32-compensated one, exactly as in the two-phase path.
+int fused_fallback(Handle &H, const DevTree &T, const std::vector<Launch> &launches,
+                   const std::vector<Launch> &launches64, std::vector<double *> &dev, int strategy, int64_t npts,
+                   const double *dx, const double *dy, const double *dz, RunPool P, int64_t nd)
+{
+    std::vector<uint32_t> list(nd), heavy, light;
+    std::vector<unsigned> acc(nd);
+    uint32_t *lst = reinterpret_cast<uint32_t *>(H.sched_tmp.p);
+    CK(H.sched_tmp.reserve(sizeof(uint32_t) * 2 * nd));
+    lst = H.sched_tmp.as<uint32_t>();
+    CK(cudaMemcpyAsync(lst, P.deferred, sizeof(uint32_t) * nd, cudaMemcpyDeviceToDevice, H.stream));
+    CK(cudaMemsetAsync(P.qacc, 0, sizeof(unsigned) * nd, H.stream));
+    CK(cudaMemsetAsync(P.qflag, 0, sizeof(int) * nd, H.stream));
+    P.count_only = 1;
+    if (strategy != SCATTER) CK(launch_nearest_list(&H, T, nd, lst, dx, dy, dz, P.bnear));
+    unsigned long long *ctr = H.pool_ctr.as<unsigned long long>();
+    CK(launch_walk(&H, T, strategy, P, nd, lst, dx, dy, dz, ctr + 2));
+    CK(cudaMemcpyAsync(list.data(), lst, sizeof(uint32_t) * nd, cudaMemcpyDeviceToHost, H.stream));
+    CK(cudaMemcpyAsync(acc.data(), P.qacc, sizeof(unsigned) * nd, cudaMemcpyDeviceToHost, H.stream));
+    CK(cudaStreamSynchronize(H.stream));
+    for (int64_t k = 0; k < nd; ++k) (acc[k] > (unsigned)H.light_max ? heavy : light).push_back(list[k]);
+    uint32_t *hl = lst, *ll = lst + heavy.size();
+    if (!heavy.empty())
+        CK(cudaMemcpyAsync(hl, heavy.data(), sizeof(uint32_t) * heavy.size(), cudaMemcpyHostToDevice, H.stream));
+    if (!light.empty())
+        CK(cudaMemcpyAsync(ll, light.data(), sizeof(uint32_t) * light.size(), cudaMemcpyHostToDevice, H.stream));
+    if (!heavy.empty())
+        for (const Launch &Lc : launches) {
+            DevCatalog C = dev_catalog(H, Lc, dev.data());
+            CK(launch_points_fp32(&H, T, C, strategy, (int64_t)heavy.size(), dx, dy, dz, hl, npts));
+            H.interp_launches++;
+        }
+    if (!light.empty())
+        for (const Launch &Lc : launches64) {
+            DevCatalog C = dev_catalog(H, Lc, dev.data());
+            CK(launch_points_fp64(&H, T, C, strategy, (int64_t)light.size(), dx, dy, dz, ll, npts));
+            H.interp_launches++;
+        }
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
+
 // FP32-compensated points in two phases: the walk kernels write every (query, subtree) item's
 // accepted runs, the pair kernel evaluates them (once per catalog launch).  Queries go through
 // in slices of H.slice (Morton order when sorted), which bounds the item and pool memory.
@@ -510,9 +554,9 @@ int reserve_pool(Handle &H, int64_t m, int ns)
 //   1 tuned:   Morton order, walk split into ~walk_split subtrees, pairs heaviest first;
 //   2 learned: as tuned, with the walk order binned by the MLP's predicted work
 //              (heaviest class first, Morton order inside a class).
-int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &launches, std::vector<double *> &dev,
-                     int strategy, int64_t npts, const double *dx, const double *dy, const double *dz,
-                     const uint32_t *perm)
+int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &launches,
+                     const std::vector<Launch> &launches64, std::vector<double *> &dev, int strategy, int64_t npts,
+                     const double *dx, const double *dy, const double *dz, const uint32_t *perm)
 {
     if (npts > 0x7fffffffLL) return fail(H, PB_ERR_CAPACITY, "more than 2^31-1 sample points in one call");
     const int mode = H.sched;
@@ -563,6 +607,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             P.qflag = H.qflag.as<int>();
             P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
             P.deferred = lists[round & 1];
+            P.count_only = 0;
             if (round == 0) ev_record(H, 4);
             if (strategy != SCATTER || mode == 2) {
                 CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
@@ -587,13 +632,21 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
             H.interp_launches++;
             uint32_t *order = nullptr;
-            if (mode != 0) CK(launch_lpt_order(&H, P, m, &order));
+            int64_t m_heavy = 0;
+            CK(launch_split_order(&H, P, m, (unsigned)H.light_max, mode == 0, &order, &m_heavy));
             if (round == 0) ev_record(H, 6);
-            for (const Launch &Lc : launches) {
-                DevCatalog C = dev_catalog(H, Lc, dev.data());
-                CK(launch_pairs_fp32(&H, T, C, strategy, P, m, ql, order, dx, dy, dz));
-                H.interp_launches++;
-            }
+            if (m_heavy > 0)
+                for (const Launch &Lc : launches) {
+                    DevCatalog C = dev_catalog(H, Lc, dev.data());
+                    CK(launch_pairs_fp32(&H, T, C, strategy, P, m_heavy, ql, order, dx, dy, dz));
+                    H.interp_launches++;
+                }
+            if (m_heavy < m)
+                for (const Launch &Lc : launches64) {   // light queries: FP64, the reference's arithmetic
+                    DevCatalog C = dev_catalog(H, Lc, dev.data());
+                    CK(launch_pairs_fp64(&H, T, C, strategy, P, m - m_heavy, ql, order + m_heavy, dx, dy, dz));
+                    H.interp_launches++;
+                }
             if (round == 0) ev_record(H, 7);
             unsigned nd = 0;
             CK(cudaMemcpyAsync(&nd, P.n_deferred, sizeof(unsigned), cudaMemcpyDeviceToHost, H.stream));
@@ -604,11 +657,8 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             if (nd == 0) break;
             H.deferred_total += nd;
             if ((int64_t)nd > m - m / 8) {   // under 1/8 of the queries completed: finish them fused
-                for (const Launch &Lc : launches) {
-                    DevCatalog C = dev_catalog(H, Lc, dev.data());
-                    CK(launch_points_fp32(&H, T, C, strategy, nd, dx, dy, dz, P.deferred, npts));
-                    H.interp_launches++;
-                }
+                int rc2 = fused_fallback(H, T, launches, launches64, dev, strategy, npts, dx, dy, dz, P, nd);
+                if (rc2) return rc2;
                 break;
             }
             // the deferred list is walked next; in learned mode it is binned again
@@ -650,14 +700,15 @@ int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, 
     if ((rc = query_order(H, npts, dx, dy, dz, &perm))) return rc;
     DevTree T = make_tree(H);
     std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
+    std::vector<Launch> launches64 = plan(items_of(cat, false));
     ev_record(H, 2);
     if (precision == PB_FP64) {
-        for (const Launch &Lc : launches) {
+        for (const Launch &Lc : launches64) {
             DevCatalog C = dev_catalog(H, Lc, dev.data());
-            CK(launch_points_fp64(&H, T, C, strategy, npts, dx, dy, dz, perm));
+            CK(launch_points_fp64(&H, T, C, strategy, npts, dx, dy, dz, perm, npts));
             H.interp_launches++;
         }
-    } else if ((rc = two_phase_points(H, T, launches, dev, strategy, npts, dx, dy, dz, perm))) {
+    } else if ((rc = two_phase_points(H, T, launches, launches64, dev, strategy, npts, dx, dy, dz, perm))) {
         return rc;
     }
     ev_record(H, 3);
@@ -788,6 +839,9 @@ int32_t pb_set_option(pb_handle *h, const char *name, int64_t value)
     else if (!strcmp(name, "schedule")) {
         if (value < 0 || value > 2) return fail(H, PB_ERR_INVALID, "schedule must be 0 (plain), 1 (tuned) or 2 (learned)");
         H.sched = (int)value;
+    } else if (!strcmp(name, "fp64_light_max")) {
+        if (value < 0 || value > 0x7fffffffLL) return fail(H, PB_ERR_INVALID, "fp64_light_max out of range");
+        H.light_max = value;
     } else if (!strcmp(name, "slice_queries")) {
         if (value < 1024) return fail(H, PB_ERR_INVALID, "slice_queries must be >= 1024");
         H.slice = value;

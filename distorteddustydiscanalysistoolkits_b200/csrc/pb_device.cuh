@@ -79,6 +79,7 @@ struct RunPool {
     int *qflag;                   // 1: some item of the query found the pool full (deferred)
     unsigned *n_deferred;         // queries deferred in this walk
     uint32_t *deferred;           // their query indices
+    int count_only;               // 1: only count accepted leaves (qacc); no runs, no items
 };
 
 // Catalog of one launch.  ucol[] are the unique sorted quantity columns read per

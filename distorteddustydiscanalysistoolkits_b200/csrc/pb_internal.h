@@ -76,6 +76,7 @@ struct Handle {
         lpt_va, iota;
     int walk_split = 64;   // target number of subtrees each query's walk is split into
     int sched = 1;         // 0 plain (input order, one walk per query, no ordering), 1 tuned, 2 learned
+    int64_t light_max = 4096;   // FP32C: queries with at most this many neighbours are summed in FP64
     int64_t slice = int64_t(1) << 22;   // queries per two-phase slice
     // learned work prediction (pb_sched.cu)
     DBuf mlp_w, mlp_m, mlp_v, mlp_g, mlp_norm, mlp_scr, mlp_idx, mlp_x, mlp_y, mlp_loss, sched_feat, sched_pred,
@@ -124,6 +125,8 @@ cudaError_t launch_nearest_list(Handle *H, const DevTree &T, int64_t m, const ui
 cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m, const uint32_t *ql,
                         const double *qx, const double *qy, const double *qz, unsigned long long *counter);
 cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order);
+cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned light_max, bool plain,
+                               uint32_t **order, int64_t *m_heavy);
 cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out);
 
 // ---- launchers (pb_sched.cu) ----
@@ -144,7 +147,11 @@ cudaError_t launch_pairs_fp32(Handle *H, const DevTree &T, const DevCatalog &C, 
                               int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
                               const double *qy, const double *qz);
 cudaError_t launch_points_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
-                               const double *qx, const double *qy, const double *qz, const uint32_t *perm);
+                               const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                               int64_t npts);
+cudaError_t launch_pairs_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, const RunPool &P,
+                              int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                              const double *qy, const double *qz);
 cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
                                const double *qx, const double *qy, const double *qz, const uint32_t *perm,
                                int64_t npts);

@@ -484,7 +484,6 @@ __global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, co
     const int lane = threadIdx.x & 31;
     const float sig = ldexp_norm3(KT);
     const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
-    const int ns = P.ns;
     for (;;) {
         int64_t t = next_query(counter, lane);
         if (t >= m) break;
@@ -495,97 +494,28 @@ __global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, co
         Query32 Q;
         Acc32 A;
         setup32<STRAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride);
-        int fill = 0, nb = 0;   // nb: full batches since the last flush (warp-uniform)
+        int nb = 0;   // full batches since the last flush (warp-uniform)
         int64_t mine = -1;
-        for (int s0 = 0; s0 < ns; s0 += 32) {
-            const int2 itm = s0 + lane < ns ? __ldg(P.items + j * ns + s0 + lane) : make_int2(-1, 0);
-            unsigned nonempty = __ballot_sync(0xffffffffu, itm.y > 0);
-            while (nonempty) {
-                const int l = __ffs(nonempty) - 1;
-                nonempty &= nonempty - 1;
-                int c = __shfl_sync(0xffffffffu, itm.x, l);
-                int left = __shfl_sync(0xffffffffu, itm.y, l);
-                if (!A.have) offsets_from(A, pay, stride, __ldg(&P.runs[(int64_t)c * RUN_CHUNK].x));
-                while (left > 0) {
-                    const int cnt = left < RUN_CHUNK ? left : RUN_CHUNK;
-                    const uint2 rn = lane < cnt ? __ldg(P.runs + (int64_t)c * RUN_CHUNK + lane) : make_uint2(0u, 0u);
-                    const int nextc = left > RUN_CHUNK ? __ldg(P.next + c) : -1;
-                    unsigned inc = rn.y;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
-                        if (lane >= o) inc += v;
-                    }
-                    const int64_t tot = __shfl_sync(0xffffffffu, inc, 31);
-                    const unsigned ex_own = inc - rn.y;
-                    int64_t tb = -fill;
-                    // uniform cursor: run r0 holds leaf position max(tb, 0) of the chunk; a batch
-                    // inside one run needs no search
-                    int r0 = -1, rc = -1;
-                    unsigned end0 = 0, lo0 = 0, ex0 = 0;
-                    for (;;) {
-                        // t0 < tot = inc[cnt - 1], so the cursor stops at a run of this chunk
-                        const unsigned t0 = tb <= 0 ? 0u : (tb < tot ? (unsigned)tb : (unsigned)(tot - 1));
-                        while (end0 <= t0 && r0 < 31) {
-                            ++r0;
-                            end0 = __shfl_sync(0xffffffffu, inc, r0);
-                        }
-                        if ((nb & 1) == 0 && tb >= 0 && tb + 64 <= (int64_t)end0) {
-                            // two full batches inside one run, flush boundary after the second
-                            if (rc != r0) {
-                                lo0 = __shfl_sync(0xffffffffu, rn.x, r0);
-                                ex0 = __shfl_sync(0xffffffffu, ex_own, r0);
-                                rc = r0;
-                            }
-                            const int64_t m1 = (int64_t)lo0 + ((unsigned)tb - ex0) + lane;
-                            pair32x2<STRAT, KT>(A, C, need_grad, Q, pay, stride, m1, m1 + 32);
-                            nb += 2;
-                            if (nb == CHUNK) {
-                                A.flush(C, need_grad);
-                                nb = 0;
-                            }
-                            tb += 64;
-                            continue;   // the next pass assigns or closes what is left of the chunk
-                        }
-                        if (tb >= 0 && tb + 32 <= (int64_t)end0) {
-                            if (rc != r0) {
-                                lo0 = __shfl_sync(0xffffffffu, rn.x, r0);
-                                ex0 = __shfl_sync(0xffffffffu, ex_own, r0);
-                                rc = r0;
-                            }
-                            mine = (int64_t)lo0 + ((unsigned)tb - ex0) + lane;
-                        } else {
-                            const int64_t tl = tb + lane;
-                            const bool here = tl >= 0 && tl < tot;
-                            const unsigned tt = here ? (unsigned)tl : 0u;
-                            int r = 0;
-#pragma unroll
-                            for (int sh = 16; sh > 0; sh >>= 1) {
-                                unsigned v = __shfl_sync(0xffffffffu, inc, r + sh - 1);
-                                if (v <= tt) r += sh;
-                            }
-                            const unsigned lo = __shfl_sync(0xffffffffu, rn.x, r);
-                            const unsigned ex = __shfl_sync(0xffffffffu, ex_own, r);
-                            if (here) mine = (int64_t)lo + (tt - ex);
-                        }
-                        if (tb + 31 < tot) {
-                            pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);   // full batch
-                            if (++nb == CHUNK) {
-                                A.flush(C, need_grad);
-                                nb = 0;
-                            }
-                            mine = -1;
-                            tb += 32;
-                        } else {
-                            fill = (int)(tot - tb);
-                            break;
-                        }
-                    }
-                    left -= cnt;
-                    c = nextc;
-                }
+        auto first = [&](int64_t b0) {
+            if (!A.have) offsets_from(A, pay, stride, b0);
+        };
+        auto one = [&](int64_t b) {
+            pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, b);
+            if (++nb == CHUNK) {
+                A.flush(C, need_grad);
+                nb = 0;
             }
-        }
+        };
+        auto two = [&](int64_t m1) {   // flush boundary after the second batch (nb is even here)
+            pair32x2<STRAT, KT>(A, C, need_grad, Q, pay, stride, m1, m1 + 32);
+            nb += 2;
+            if (nb == CHUNK) {
+                A.flush(C, need_grad);
+                nb = 0;
+            }
+        };
+        auto cantwo = [&]() { return (nb & 1) == 0; };
+        deal_runs(P, j, lane, first, one, two, cantwo, mine);
         if (mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);
         reduce_finalize32(A, C, need_grad, qi, lane);
     }

@@ -98,7 +98,8 @@ __device__ __forceinline__ void finalize64(const double *v, const DevCatalog &C,
 template <int STRAT>
 __global__ void __launch_bounds__(128) k_points64w(DevTree T, DevCatalog C, int64_t nq, const double *__restrict__ qx,
                                                    const double *__restrict__ qy, const double *__restrict__ qz,
-                                                   const uint32_t *__restrict__ perm, unsigned long long *counter)
+                                                   const uint32_t *__restrict__ perm, int64_t npts,
+                                                   unsigned long long *counter)
 {
     __shared__ double sterm[4][32][NT + 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(128) k_points64w(DevTree T, DevCatalog C, int6
         int64_t j = next_query(counter, lane);
         if (j >= nq) break;
         int64_t qi = perm ? (int64_t)__ldg(perm + j) : j;
-        if (qi >= nq) continue;
+        if (qi >= npts) continue;
         double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
         double ha = 0.0;
         if (STRAT != SCATTER) {
@@ -148,6 +149,60 @@ __global__ void __launch_bounds__(128) k_points64w(DevTree T, DevCatalog C, int6
     }
 }
 
+// Two-phase form: the warp reads the walked query's runs (deal_runs) instead of walking, with
+// the same per-slot terms and the same in-order column sums, so the values are those of
+// k_points64w bit for bit.
+template <int STRAT>
+__global__ void __launch_bounds__(128) k_pairs64w(DevTree T, DevCatalog C, RunPool P, int64_t m,
+                                                  const uint32_t *__restrict__ ql, const uint32_t *__restrict__ order,
+                                                  const double *__restrict__ qx, const double *__restrict__ qy,
+                                                  const double *__restrict__ qz, unsigned long long *counter)
+{
+    __shared__ double sterm[4][32][NT + 1];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
+    for (;;) {
+        int64_t t = next_query(counter, lane);
+        if (t >= m) break;
+        const int64_t j = order ? (int64_t)__ldg(order + t) : t;
+        if (__ldg(P.qflag + j)) continue;
+        const int64_t qi = __ldg(ql + j);
+        const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        double ha = 0.0;
+        if (STRAT != SCATTER) {
+            const int b = __ldg(P.bnear + j);
+            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
+        }
+        double acc = 0.0;   // lane a < NT owns accumulator a
+        auto proc = [&](int fill, int64_t b) {
+            if (b >= 0) {
+                double tv[NT];
+                terms64<STRAT>(T, C, need_grad, px, py, pz, b, ha, tv);
+#pragma unroll
+                for (int a = 0; a < NT; ++a) sterm[wib][lane][a] = tv[a];
+            }
+            __syncwarp();
+            if (lane < NT)
+                for (int s = 0; s < fill; ++s) acc += sterm[wib][s][lane];
+            __syncwarp();
+        };
+        auto first = [&](int64_t) {};
+        auto one = [&](int64_t b) { proc(32, b); };
+        auto two = [&](int64_t m1) {
+            proc(32, m1);
+            proc(32, m1 + 32);
+        };
+        auto cantwo = [&]() { return false; };
+        int64_t mine = -1;
+        const int fill = deal_runs(P, j, lane, first, one, two, cantwo, mine);
+        if (fill > 0) proc(fill, mine);
+        double v[NT];
+#pragma unroll
+        for (int a = 0; a < NT; ++a) v[a] = __shfl_sync(0xffffffffu, acc, a);
+        if (lane == 0) finalize64(v, C, qi);
+    }
+}
+
 static int persistent_grid(const void *kern, int bs)
 {
     int dev = 0, sms = 148, per = 1;
@@ -158,7 +213,8 @@ static int persistent_grid(const void *kern, int bs)
 }
 
 cudaError_t launch_points_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, int64_t nq,
-                               const double *qx, const double *qy, const double *qz, const uint32_t *perm)
+                               const double *qx, const double *qy, const double *qz, const uint32_t *perm,
+                               int64_t npts)
 {
     int bs = 128;
     cudaError_t e = H->counter.reserve(sizeof(unsigned long long));
@@ -168,15 +224,42 @@ cudaError_t launch_points_fp64(Handle *H, const DevTree &T, const DevCatalog &C,
     switch (strategy) {
     case GATHER:
         k_points64w<GATHER><<<persistent_grid((const void *)k_points64w<GATHER>, bs), bs, 0, H->stream>>>(
-            T, C, nq, qx, qy, qz, perm, ctr);
+            T, C, nq, qx, qy, qz, perm, npts, ctr);
         break;
     case SCATTER:
         k_points64w<SCATTER><<<persistent_grid((const void *)k_points64w<SCATTER>, bs), bs, 0, H->stream>>>(
-            T, C, nq, qx, qy, qz, perm, ctr);
+            T, C, nq, qx, qy, qz, perm, npts, ctr);
         break;
     default:
         k_points64w<SYMMETRIC><<<persistent_grid((const void *)k_points64w<SYMMETRIC>, bs), bs, 0, H->stream>>>(
-            T, C, nq, qx, qy, qz, perm, ctr);
+            T, C, nq, qx, qy, qz, perm, npts, ctr);
+        break;
+    }
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pairs_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int strategy, const RunPool &P,
+                              int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                              const double *qy, const double *qz)
+{
+    int bs = 128;
+    cudaError_t e = H->counter.reserve(sizeof(unsigned long long));
+    if (e) return e;
+    unsigned long long *ctr = H->counter.as<unsigned long long>();
+    cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), H->stream);
+    switch (strategy) {
+    case GATHER:
+        k_pairs64w<GATHER><<<persistent_grid((const void *)k_pairs64w<GATHER>, bs), bs, 0, H->stream>>>(
+            T, C, P, m, ql, order, qx, qy, qz, ctr);
+        break;
+    case SCATTER:
+        k_pairs64w<SCATTER><<<persistent_grid((const void *)k_pairs64w<SCATTER>, bs), bs, 0, H->stream>>>(
+            T, C, P, m, ql, order, qx, qy, qz, ctr);
+        break;
+    default:
+        k_pairs64w<SYMMETRIC><<<persistent_grid((const void *)k_pairs64w<SYMMETRIC>, bs), bs, 0, H->stream>>>(
+            T, C, P, m, ql, order, qx, qy, qz, ctr);
         break;
     }
     H->launches += 1;

@@ -91,6 +91,10 @@ struct RunWriter {
 
     __device__ __forceinline__ bool store(const RunPool &P)
     {
+        if (P.count_only) {
+            ++nruns;
+            return true;
+        }
         if (cur < 0 || k == RUN_CHUNK) {
             int c = alloc_chunk(P);
             if (c < 0) return false;
@@ -139,8 +143,8 @@ __global__ void __launch_bounds__(128) k_walk_items(DevTree T, RunPool P, int64_
         const int s = (int)(wi % ns);
         if (j >= m) continue;
         const uint32_t qi = __ldg(ql + j);
-        bool ok = *(volatile unsigned long long *)P.used < P.cap &&
-                  *(volatile int *)(P.qflag + j) == 0;   // pool exhausted or query already deferred
+        bool ok = P.count_only || (*(volatile unsigned long long *)P.used < P.cap &&
+                                   *(volatile int *)(P.qflag + j) == 0);   // pool exhausted or query deferred
         RunWriter R;
         if (ok) {
             const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
@@ -163,6 +167,10 @@ __global__ void __launch_bounds__(128) k_walk_items(DevTree T, RunPool P, int64_
             if (ok) ok = R.close(P);
         }
         const int64_t it = j * ns + s;
+        if (P.count_only) {
+            if (R.nacc > 0) atomicAdd(P.qacc + j, (unsigned)R.nacc);
+            continue;
+        }
         if (!ok) {
             P.items[it] = make_int2(RUN_DEFERRED, 0);
             if (atomicExch(P.qflag + j, 1) == 0) {
@@ -183,6 +191,28 @@ __global__ void k_lpt_keys(int64_t m, const unsigned *__restrict__ qacc, const i
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
         unsigned a = qflag[j] ? 0u : qacc[j];
         keys[j] = 0x7fffffffu - (a > 0x7fffffffu ? 0x7fffffffu : a);
+        vals[j] = (uint32_t)j;
+    }
+}
+
+// queries (not deferred) with more than `light_max` accepted leaves; one atomic per block
+__global__ void k_count_heavy(int64_t m, const unsigned *__restrict__ qacc, const int *__restrict__ qflag,
+                              unsigned light_max, unsigned *count)
+{
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < m; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = base + threadIdx.x;
+        const int heavy = j < m && !qflag[j] && qacc[j] > light_max;
+        const int c = __syncthreads_count(heavy);
+        if (threadIdx.x == 0 && c) atomicAdd(count, (unsigned)c);
+    }
+}
+
+// plain schedule: a stable partition, heavy queries first, input order kept in each part
+__global__ void k_heavy_keys(int64_t m, const unsigned *__restrict__ qacc, const int *__restrict__ qflag,
+                             unsigned light_max, uint32_t *keys, uint32_t *vals)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+        keys[j] = (!qflag[j] && qacc[j] > light_max) ? 0u : 1u;
         vals[j] = (uint32_t)j;
     }
 }
@@ -274,6 +304,40 @@ cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **
                             H->lpt_va.as<uint32_t>(), m, 31)))
         return e;
     *order = H->lpt_v.as<uint32_t>();
+    return cudaSuccess;
+}
+
+// pair order of a walked slice and the number of heavy queries at its front: heaviest first
+// (LPT) unless `plain`, where it is the stable heavy/light partition of the walk order
+cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned light_max, bool plain,
+                               uint32_t **order, int64_t *m_heavy)
+{
+    cudaError_t e;
+    if (!plain) {
+        if ((e = launch_lpt_order(H, P, m, order))) return e;
+    } else {
+        if ((e = H->lpt_k.reserve(4 * m))) return e;
+        if ((e = H->lpt_v.reserve(4 * m))) return e;
+        if ((e = H->lpt_ka.reserve(4 * m))) return e;
+        if ((e = H->lpt_va.reserve(4 * m))) return e;
+        k_heavy_keys<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, light_max, H->lpt_k.as<uint32_t>(),
+                                                             H->lpt_v.as<uint32_t>());
+        H->launches += 1;
+        if ((e = cudaGetLastError())) return e;
+        if ((e = sort_pairs_u32(H, H->lpt_k.as<uint32_t>(), H->lpt_v.as<uint32_t>(), H->lpt_ka.as<uint32_t>(),
+                                H->lpt_va.as<uint32_t>(), m, 1)))
+            return e;
+        *order = H->lpt_v.as<uint32_t>();
+    }
+    unsigned *cnt = reinterpret_cast<unsigned *>(P.n_deferred) + 1;
+    if ((e = cudaMemsetAsync(cnt, 0, sizeof(unsigned), H->stream))) return e;
+    k_count_heavy<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, light_max, cnt);
+    H->launches += 1;
+    if ((e = cudaGetLastError())) return e;
+    unsigned hcount = 0;
+    if ((e = cudaMemcpyAsync(&hcount, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, H->stream))) return e;
+    if ((e = cudaStreamSynchronize(H->stream))) return e;
+    *m_heavy = hcount;
     return cudaSuccess;
 }
 

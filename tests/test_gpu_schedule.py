@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 COLS = ("rho", "vx", "vy", "vz")
 
 
-def _run(p, flat, strategy, options=(), env=None):
+def _run(p, flat, strategy, options=(), env=None, precision=pb.FP32C):
     old = {k: os.environ.get(k) for k in ("PB_RUN_POOL_CHUNKS", "PB_RUN_POOL_MB")}
     for k in old:
         os.environ.pop(k, None)
@@ -31,7 +31,7 @@ def _run(p, flat, strategy, options=(), env=None):
         inp = pb.InterpolationInput(p["x"].copy(), p["y"].copy(), p["z"].copy(), p["m"].copy(), p["h"].copy(),
                                     p["rho"].copy(), tuple(p[c].copy() for c in COLS))
         cat = pb.InterpolationCatalog(COLS, **synthetic.C2_CATALOG)
-        out = pb.PointSamples_interpolation(be, flat, inp, cat, strategy, precision=pb.FP32C)
+        out = pb.PointSamples_interpolation(be, flat, inp, cat, strategy, precision=precision)
         return np.stack([g.grid for g in out.grids]), be.handle.schedule()
     finally:
         be.close()
@@ -72,3 +72,25 @@ def test_fp32c_identical_across_schedules(case, strategy):
     got, (rounds, deferred, _) = _run(p, flat, strategy, env={"PB_RUN_POOL_CHUNKS": "1"})
     assert deferred > 0
     _same_bits(got, ref)
+
+
+@pytest.mark.parametrize("strategy", [pb.itpGather, pb.itpSymmetric])
+def test_light_queries_are_summed_exactly_in_fp64(case, strategy):
+    """FP32C mode sums queries with at most 4096 accepted neighbours (option fp64_light_max) with
+    the FP64 kernels: their values are the FP64 mode's, bit for bit."""
+    p, flat = case
+    got, _ = _run(p, flat, strategy)
+    exact, _ = _run(p, flat, strategy, precision=pb.FP64)
+    be = pb.CUDAComputeBackend(0)
+    try:
+        inp = pb.InterpolationInput(p["x"], p["y"], p["z"], p["m"], p["h"], p["rho"], ())
+        lb = pb.LinearBVH_build(inp, be)
+        acc = pb.traversal_stats(lb, flat.coor, strategy)[:, 4]
+    finally:
+        be.close()
+    light = acc <= 4096
+    assert light.any() and (~light).any()
+    assert np.array_equal(got[:, light].view(np.uint64), exact[:, light].view(np.uint64))
+    alt, _ = _run(p, flat, strategy, options=(("fp64_light_max", 0),))
+    nonempty = light & (acc > 0)
+    assert not np.array_equal(alt[:, nonempty].view(np.uint64), exact[:, nonempty].view(np.uint64))
