@@ -448,7 +448,7 @@ int do_build(Handle &H, const pb_input *in, int32_t flags)
 }
 
 // Run pool of the two-phase point path.  Its size follows the number of queries (24 chunks
-// of 32 runs per query), bounded by a sixth of the device memory (at most 24 GiB), by
+// of 32 runs per query), bounded by half of the free device memory (at most 64 GiB), by
 // PB_RUN_POOL_MB, or set exactly in chunks by PB_RUN_POOL_CHUNKS; it never drops below what
 // one query can need (n/2 runs) unless one of the two variables asks for less.  Buffers only
 // grow; the cap of a call is what it may use.
@@ -465,10 +465,11 @@ int reserve_pool(Handle &H, int64_t m, int ns)
     unsigned long long budget;
     if (env_mb > 0) budget = (unsigned long long)env_mb << 20;
     else {
+        // half of the free memory plus what the pool already holds, at most 64 GiB
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        budget = tot / 6;
-        if (budget > (24ULL << 30)) budget = 24ULL << 30;
+        budget = (fr + H.pool_runs.bytes + H.pool_next.bytes) / 2;
+        if (budget > (64ULL << 30)) budget = 64ULL << 30;
     }
     unsigned long long cap = budget / per_chunk;
     if (cap > want) cap = want;
@@ -542,6 +543,37 @@ int fused_fallback(Handle &H, const DevTree &T, const std::vector<Launch> &launc
     return PB_OK;
 }
 
+// Doubles the run pool (within the budget of reserve_pool) after a round that deferred
+// queries; the pool is empty between rounds, so nothing is lost.  Returns false if it cannot
+// grow (at the budget, fixed by PB_RUN_POOL_CHUNKS, or out of memory).
+bool grow_pool(Handle &H)
+{
+    if (getenv("PB_RUN_POOL_CHUNKS") || getenv("PB_RUN_POOL_MB")) return false;
+    const unsigned long long per_chunk = sizeof(uint2) * RUN_CHUNK + sizeof(int);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return false;
+    unsigned long long budget = (fr + H.pool_runs.bytes + H.pool_next.bytes) / 2;
+    if (budget > (64ULL << 30)) budget = 64ULL << 30;
+    unsigned long long cap = std::min<unsigned long long>(2 * H.pool_cap, budget / per_chunk);
+    if (cap > 0x7fffffffULL) cap = 0x7fffffffULL;
+    if (cap <= H.pool_cap) return false;
+    H.pool_runs.release();
+    H.pool_next.release();
+    if (H.pool_runs.reserve(sizeof(uint2) * RUN_CHUNK * cap) || H.pool_next.reserve(sizeof(int) * cap)) {
+        cudaGetLastError();
+        H.pool_runs.release();
+        H.pool_next.release();
+        cap = H.pool_cap;   // fall back to the old size
+        if (H.pool_runs.reserve(sizeof(uint2) * RUN_CHUNK * cap) || H.pool_next.reserve(sizeof(int) * cap)) {
+            cudaGetLastError();
+            H.pool_cap = 0;
+        }
+        return false;
+    }
+    H.pool_cap = cap;
+    return true;
+}
+
 // FP32-compensated points in two phases: the walk kernels write every (query, subtree) item's
 // accepted runs, the pair kernel evaluates them (once per catalog launch).  Queries go through
 // in slices of H.slice (Morton order when sorted), which bounds the item and pool memory.
@@ -587,9 +619,11 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
     H.walk_rounds = 0;
     H.deferred_total = 0;
     for (int k = 0; k < 3; ++k) H.t_phase_ms[k] = 0.f;
-    for (int64_t s0 = 0; s0 < npts; s0 += S) {
+    int64_t Snext = S;   // slice size, adapted to the pool use seen so far
+    for (int64_t s0 = 0; s0 < npts;) {
         const uint32_t *ql = ql_all + s0;
-        int64_t m = std::min<int64_t>(S, npts - s0);
+        int64_t m = std::min<int64_t>(Snext, npts - s0);
+        s0 += m;
         for (int round = 0;; ++round) {
             CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
             CK(cudaMemsetAsync(H.qacc.p, 0, sizeof(unsigned) * m, H.stream));
@@ -648,15 +682,34 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                     H.interp_launches++;
                 }
             if (round == 0) ev_record(H, 7);
-            unsigned nd = 0;
-            CK(cudaMemcpyAsync(&nd, P.n_deferred, sizeof(unsigned), cudaMemcpyDeviceToHost, H.stream));
+            unsigned long long used_nd[2] = {0, 0};
+            CK(cudaMemcpyAsync(used_nd, ctr, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, H.stream));
             CK(cudaStreamSynchronize(H.stream));
+            const unsigned nd = (unsigned)(used_nd[1] & 0xffffffffULL);
+            if (round == 0) {
+                // next slice: the queries that 85 % of the pool holds at this slice's chunks per query
+                const unsigned long long used = std::min<unsigned long long>(used_nd[0], H.pool_cap);
+                const int64_t done = m - (int64_t)nd;
+                if (done > 0 && used > 0) {
+                    const double per = (double)used / (double)done;
+                    Snext = std::max<int64_t>(1024, std::min<int64_t>(S, (int64_t)(0.85 * (double)H.pool_cap / per)));
+                } else if (nd > 0) {
+                    Snext = std::max<int64_t>(1024, Snext / 2);
+                }
+            }
             if (round == 0)
                 for (int k = 0; k < 3; ++k) H.t_phase_ms[k] += ev_ms(H, 4 + k, 5 + k);
             H.walk_rounds = std::max<int64_t>(H.walk_rounds, round + 1);
             if (nd == 0) break;
             H.deferred_total += nd;
-            if ((int64_t)nd > m - m / 8) {   // under 1/8 of the queries completed: finish them fused
+            const bool grew = grow_pool(H);
+            if (grew) {
+                // the bigger pool holds proportionally more of a slice
+                Snext = std::min<int64_t>(S, Snext * 2);
+            } else if (H.pool_cap == 0) {
+                return fail(H, PB_ERR_CUDA, "run pool could not be reallocated");
+            }
+            if (!grew && (int64_t)nd > m - m / 8) {   // under 1/8 completed, pool at its limit: finish fused
                 int rc2 = fused_fallback(H, T, launches, launches64, dev, strategy, npts, dx, dy, dz, P, nd);
                 if (rc2) return rc2;
                 break;
