@@ -9,7 +9,10 @@ in FP32 with compensated accumulation (FP64 distance tests and pair offsets).
 
 One step = one pass of the hot path over the snapshot with inputs resident in HBM:
 LinearBVH! (quantise, encode, radix sort, dedupe, gather, topology, refit) followed by the
-fused nearest-h + symmetric traversal + kernel sums for every grid point.
+interpolation of every grid point: nearest-h search, symmetric walk emitting accepted runs,
+kernel sums over the runs (FP32 compensated; FP64 for queries with <= 4096 neighbours).
+--config c5 runs the clumped 16M-particle disc (C4 Wendland, rho + curl v, 256^3 grid);
+"schedules" compares the plain, tuned and learned query schedules (identical outputs).
   value     grid points / s of the interpolation stage (build excluded; CUDA events on
             the launching stream), summed over ranks (weak scaling: one snapshot per GPU)
   build_ms  LBVH build time per step (CUDA events)
@@ -340,8 +343,8 @@ def main():
                 schedules[name]["speedup_vs_plain"] = schedules["plain"]["interp_ms"] / schedules[name]["interp_ms"]
         phases.clear()
 
-    # roofline of the dominant kernel phase (FP32C: walk kernels vs pair kernel, per-phase CUDA
-    # events of the library; FP64: the fused kernel)
+    # roofline of the dominant kernel phase (walk kernels vs pair kernels, per-phase CUDA events
+    # of the library)
     lb = pb.LinearBVH(backend, nparticles)
     roofline = None
     if not args.no_roofline:
@@ -352,21 +355,17 @@ def main():
             os.path.join(REPO, "MEASURED_PEAKS.json")) else None
         peak = peaks["hbm_gbs"] if peaks else 6650.0
         ph = np.mean(np.array(main_phases), axis=0) if main_phases else np.zeros(3)
-        if prec == pb.FP32C:
-            kname = {"M4_spline": "M4", "C4_Wendland": "C4"}.get(config["kernel"], config["kernel"])
-            kern = {"walk": ("k_nearest_list + k_walk_items<itpSymmetric>", ph[0] + ph[1]),
-                    "pairs": ("k_pairs32w<itpSymmetric,%s>" % kname, ph[2])}
-        else:
-            kern = {"fused": ("k_points64w<itpSymmetric>", interp_ms)}
-            alg = {"fused": alg["walk"] + alg["pairs"]}
+        kname = {"M4_spline": "M4", "C4_Wendland": "C4"}.get(config["kernel"], config["kernel"])
+        pk = "k_pairs32w<itpSymmetric,%s> (+ k_pairs64w for light queries)" % kname if prec == pb.FP32C \
+            else "k_pairs64w<itpSymmetric>"
+        kern = {"walk": ("k_nearest_list + k_walk_items<itpSymmetric>", ph[0] + ph[1]), "pairs": (pk, ph[2])}
         per = {}
         for key, (name, ms) in kern.items():
             a = alg[key] / (ms / 1e3) / 1e9 if ms > 0 else None
             per[key] = {"kernel": name, "ms": float(ms), "algorithmic_bytes": alg[key], "achieved_gbs": a}
         dom = max(per, key=lambda k: per[k]["ms"])
         traffic = None
-        prof = os.path.join(REPO, "profiles", {"pairs": "k_pairs32w", "walk": "k_walk_items",
-                                                "fused": "k_points64w"}[dom] + "_c2_traffic.json")
+        prof = os.path.join(REPO, "profiles", {"pairs": "k_pairs32w", "walk": "k_walk_items"}[dom] + "_c2_traffic.json")
         if os.path.exists(prof) and args.precision == "fp32c" and args.config == "c2" and \
                 args.particles in (None, 1 << 21) and args.grid in (None, "256,256,64"):
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")

@@ -756,11 +756,12 @@ int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, 
     std::vector<Launch> launches64 = plan(items_of(cat, false));
     ev_record(H, 2);
     if (precision == PB_FP64) {
-        for (const Launch &Lc : launches64) {
-            DevCatalog C = dev_catalog(H, Lc, dev.data());
-            CK(launch_points_fp64(&H, T, C, strategy, npts, dx, dy, dz, perm, npts));
-            H.interp_launches++;
-        }
+        // every query summed by the FP64 pair kernel (the fused kernel's arithmetic, bit for bit)
+        const int64_t keep = H.light_max;
+        H.light_max = 0x7fffffffLL;
+        rc = two_phase_points(H, T, launches64, launches64, dev, strategy, npts, dx, dy, dz, perm);
+        H.light_max = keep;
+        if (rc) return rc;
     } else if ((rc = two_phase_points(H, T, launches, launches64, dev, strategy, npts, dx, dy, dz, perm))) {
         return rc;
     }
