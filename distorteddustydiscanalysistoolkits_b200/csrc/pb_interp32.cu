@@ -98,6 +98,45 @@ __device__ __forceinline__ float ldexp_norm3(int k)
 //   offset x_a - x_b is formed in FP32 as (xa_hi - xb_hi) + (xa_lo - xb_lo) without FP64 loads.
 __host__ __device__ inline int payload_stride(int nU) { return 2 + (2 + 2 * nU + 3) / 4; }
 
+// Compile-time shape of a launch's catalog, for the pair kernels.  CAT 0 reads everything from
+// the DevCatalog at run time; 1: four columns, gradient + divergence + curl; 2: four columns,
+// curl only; 3: one column, scalars only.  A specialised kernel performs exactly the
+// operations, in the same order, that the generic one performs for such a catalog.
+constexpr int CAT_ANY = 0, CAT_GDC4 = 1, CAT_C4 = 2, CAT_S1 = 3;
+
+template <int CAT>
+struct CatShape {
+    __device__ static __forceinline__ int nu(const DevCatalog &C)
+    {
+        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 4 : (CAT == CAT_S1 ? 1 : C.nU);
+    }
+    __device__ static __forceinline__ bool grad(const DevCatalog &C)
+    {
+        return CAT == CAT_GDC4 ? true : (CAT == CAT_ANY ? C.n_grad > 0 : false);
+    }
+    __device__ static __forceinline__ bool div(const DevCatalog &C)
+    {
+        return CAT == CAT_GDC4 ? true : (CAT == CAT_ANY ? C.n_div > 0 : false);
+    }
+    __device__ static __forceinline__ bool curl(const DevCatalog &C)
+    {
+        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? true : (CAT == CAT_ANY ? C.n_curl > 0 : false);
+    }
+    __device__ static __forceinline__ bool any(const DevCatalog &C) { return grad(C) || div(C) || curl(C); }
+    __device__ static __forceinline__ int stride(int s)
+    {
+        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 5 : (CAT == CAT_S1 ? 3 : s);
+    }
+};
+
+inline int catalog_shape(const DevCatalog &C)
+{
+    if (C.nU == 4 && C.n_grad == 1 && C.g_u[0] == 0 && C.n_div == 1 && C.n_curl == 1) return CAT_GDC4;
+    if (C.nU == 4 && C.n_grad == 0 && C.n_div == 0 && C.n_curl == 1) return CAT_C4;
+    if (C.nU == 1 && C.n_grad == 0 && C.n_div == 0 && C.n_curl == 0) return CAT_S1;
+    return CAT_ANY;
+}
+
 __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int stride)
 {
     const float sig = ldexp_norm3(T.kernel);
@@ -173,24 +212,20 @@ struct Acc32 {
         have = false;
     }
 
-    __device__ __forceinline__ void flush(const DevCatalog &C, bool need_grad)
+    template <int CAT>
+    __device__ __forceinline__ void flush(const DevCatalog &C)
     {
+        using S = CatShape<CAT>;
         S1.add(pS1);
 #pragma unroll
         for (int u = 0; u < MAXU; ++u)
-            if (u < C.nU) SA[u].add(pSA[u]);
-        if (need_grad) {
+            if (u < S::nu(C)) SA[u].add(pSA[u]);
+        if (S::any(C)) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) B[d].add(pB[d]);
-#pragma unroll
-            for (int j = 0; j < MAXG; ++j)
-                if (j < C.n_grad) { F[j][0].add(pF[j][0]); F[j][1].add(pF[j][1]); F[j][2].add(pF[j][2]); }
-#pragma unroll
-            for (int j = 0; j < MAXD; ++j)
-                if (j < C.n_div) D[j].add(pD[j]);
-#pragma unroll
-            for (int j = 0; j < MAXC; ++j)
-                if (j < C.n_curl) { Cc[j][0].add(pC[j][0]); Cc[j][1].add(pC[j][1]); Cc[j][2].add(pC[j][2]); }
+            if (S::grad(C)) { F[0][0].add(pF[0][0]); F[0][1].add(pF[0][1]); F[0][2].add(pF[0][2]); }
+            if (S::div(C)) D[0].add(pD[0]);
+            if (S::curl(C)) { Cc[0][0].add(pC[0][0]); Cc[0][1].add(pC[0][1]); Cc[0][2].add(pC[0][2]); }
         }
         zero_partials();
     }
@@ -202,8 +237,10 @@ struct Query32 {
 };
 
 // kernel constants and column value pairs (hi, lo) of a record
+template <int CAT>
 __device__ __forceinline__ void load_cols(const float4 *rec, int stride, float &cW, float &cG, float *ch, float *cl)
 {
+    stride = CatShape<CAT>::stride(stride);
     float v[4 * 4];
 #pragma unroll
     for (int k = 2; k < 6; ++k) {
@@ -221,17 +258,19 @@ struct Terms32 {
     float w, a[MAXU], gx, gy, gz;
 };
 
-template <int STRAT, int KT>
-__device__ __forceinline__ void terms32(const Acc32 &A, bool need_grad, const Query32 &Q,
+template <int STRAT, int KT, int CAT>
+__device__ __forceinline__ void terms32(const Acc32 &A, const DevCatalog &C, const Query32 &Q,
                                         const float4 *__restrict__ pay, int stride, int64_t b, Terms32 &t)
 {
+    stride = CatShape<CAT>::stride(stride);
+    const bool need_grad = CatShape<CAT>::any(C);
     const float4 *rec = pay + b * stride;
     const float4 p0 = __ldg(rec), p1 = __ldg(rec + 1);
     const float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
     const float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
     const float dz = (Q.ph[2] - p0.z) + (Q.pl[2] - p1.z);
     float cWb, cGb, ch[MAXU], cl[MAXU];
-    load_cols(rec, stride, cWb, cGb, ch, cl);
+    load_cols<CAT>(rec, stride, cWb, cGb, ch, cl);
     const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
     const float r = r2 * rinv;
@@ -265,7 +304,7 @@ __device__ __forceinline__ void terms32(const Acc32 &A, bool need_grad, const Qu
     const float mrho = p1.w;
     t.w = mrho * W;
 #pragma unroll
-    for (int u = 0; u < MAXU; ++u) t.a[u] = (ch[u] - A.hh[u]) + (cl[u] - A.hl[u]);
+    for (int u = 0; u < MAXU; ++u) t.a[u] = u < CatShape<CAT>::nu(C) ? (ch[u] - A.hh[u]) + (cl[u] - A.hl[u]) : 0.f;
     if (need_grad) {
         const float gq = mrho * G;
         t.gx = gq * dx;
@@ -275,20 +314,23 @@ __device__ __forceinline__ void terms32(const Acc32 &A, bool need_grad, const Qu
 }
 
 // fixed slots: the gradient's column in slot 0, the div/curl vector in slots 1..3
-__device__ __forceinline__ void accum32(Acc32 &A, const DevCatalog &C, bool need_grad, const Terms32 &t)
+template <int CAT>
+__device__ __forceinline__ void accum32(Acc32 &A, const DevCatalog &C, const Terms32 &t)
 {
+    using S = CatShape<CAT>;
     A.pS1 += t.w;
 #pragma unroll
-    for (int u = 0; u < MAXU; ++u) A.pSA[u] = fmaf(t.a[u], t.w, A.pSA[u]);
-    if (need_grad) {
+    for (int u = 0; u < MAXU; ++u)
+        if (u < S::nu(C)) A.pSA[u] = fmaf(t.a[u], t.w, A.pSA[u]);
+    if (S::any(C)) {
         A.pB[0] += t.gx; A.pB[1] += t.gy; A.pB[2] += t.gz;
-        if (C.n_grad > 0) {
+        if (S::grad(C)) {
             A.pF[0][0] = fmaf(t.gx, t.a[0], A.pF[0][0]);
             A.pF[0][1] = fmaf(t.gy, t.a[0], A.pF[0][1]);
             A.pF[0][2] = fmaf(t.gz, t.a[0], A.pF[0][2]);
         }
-        if (C.n_div > 0) A.pD[0] = fmaf(t.gz, t.a[3], fmaf(t.gy, t.a[2], fmaf(t.gx, t.a[1], A.pD[0])));
-        if (C.n_curl > 0) {
+        if (S::div(C)) A.pD[0] = fmaf(t.gz, t.a[3], fmaf(t.gy, t.a[2], fmaf(t.gx, t.a[1], A.pD[0])));
+        if (S::curl(C)) {
             A.pC[0][0] = fmaf(t.a[2], t.gz, fmaf(-t.a[3], t.gy, A.pC[0][0]));
             A.pC[0][1] = fmaf(t.a[3], t.gx, fmaf(-t.a[1], t.gz, A.pC[0][1]));
             A.pC[0][2] = fmaf(t.a[1], t.gy, fmaf(-t.a[2], t.gx, A.pC[0][2]));
@@ -296,26 +338,26 @@ __device__ __forceinline__ void accum32(Acc32 &A, const DevCatalog &C, bool need
     }
 }
 
-template <int STRAT, int KT>
-__device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
+template <int STRAT, int KT, int CAT>
+__device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, const Query32 &Q,
                                        const float4 *__restrict__ pay, int stride, int64_t b)
 {
     Terms32 t;
-    terms32<STRAT, KT>(A, need_grad, Q, pay, stride, b, t);
-    accum32(A, C, need_grad, t);
+    terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b, t);
+    accum32<CAT>(A, C, t);
 }
 
 // two pairs of one lane (consecutive in its sequence): independent terms, then accumulated
 // in order -- the same arithmetic as two pair32 calls, with twice the independent work
-template <int STRAT, int KT>
-__device__ __forceinline__ void pair32x2(Acc32 &A, const DevCatalog &C, bool need_grad, const Query32 &Q,
+template <int STRAT, int KT, int CAT>
+__device__ __forceinline__ void pair32x2(Acc32 &A, const DevCatalog &C, const Query32 &Q,
                                          const float4 *__restrict__ pay, int stride, int64_t b1, int64_t b2)
 {
     Terms32 t1, t2;
-    terms32<STRAT, KT>(A, need_grad, Q, pay, stride, b1, t1);
-    terms32<STRAT, KT>(A, need_grad, Q, pay, stride, b2, t2);
-    accum32(A, C, need_grad, t1);
-    accum32(A, C, need_grad, t2);
+    terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b1, t1);
+    terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b2, t2);
+    accum32<CAT>(A, C, t1);
+    accum32<CAT>(A, C, t2);
 }
 
 __device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, const DevCatalog &C, int64_t qi)
@@ -365,7 +407,7 @@ __device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, con
 
 // per-query constants: kernel scale factors at h_a, the query position as double-float
 // pairs, and the quantity offsets (nearest particle, else the first accepted neighbour)
-template <int STRAT>
+template <int STRAT, int CAT>
 __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, double py, double pz, int64_t bnear,
                                         Query32 &Q, Acc32 &A, const float4 *pay, int stride)
 {
@@ -385,22 +427,24 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
         // quantities enter as offsets from the nearest particle's values, which are close
         // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
         float cw_, cg_;
-        load_cols(pay + bnear * stride, stride, cw_, cg_, A.hh, A.hl);
+        load_cols<CAT>(pay + bnear * CatShape<CAT>::stride(stride), stride, cw_, cg_, A.hh, A.hl);
         A.have = true;
     }
 }
 
+template <int CAT>
 __device__ __forceinline__ void offsets_from(Acc32 &A, const float4 *pay, int stride, int64_t b0)
 {
     float cw_, cg_;
-    load_cols(pay + b0 * stride, stride, cw_, cg_, A.hh, A.hl);
+    load_cols<CAT>(pay + b0 * CatShape<CAT>::stride(stride), stride, cw_, cg_, A.hh, A.hl);
     A.have = true;
 }
 
 // flush, fixed-tree FP64 reduction of the 32 lane sums, lane 0 finalises
-__device__ __forceinline__ void reduce_finalize32(Acc32 &A, const DevCatalog &C, bool need_grad, int64_t qi, int lane)
+template <int CAT>
+__device__ __forceinline__ void reduce_finalize32(Acc32 &A, const DevCatalog &C, int64_t qi, int lane)
 {
-    A.flush(C, need_grad);
+    A.flush<CAT>(C);
     double v[15];
     v[0] = A.S1.val();
 #pragma unroll
@@ -430,7 +474,6 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
     const int64_t n = T.n;
     const double K = kernel_valid(KT);
     const float sig = ldexp_norm3(KT);
-    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
     for (;;) {
         int64_t j = next_query(counter, lane);
         if (j >= nq) break;
@@ -443,14 +486,14 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
         Query32 Q;
         Acc32 A;
-        setup32<STRAT>(T, sig, px, py, pz, bnear, Q, A, pay, stride);
+        setup32<STRAT, CAT_ANY>(T, sig, px, py, pz, bnear, Q, A, pay, stride);
         Slots S{0, -1};
         int nb = 0;   // full batches since the last flush (warp-uniform)
         auto proc = [&](int fill) {
-            if (!A.have) offsets_from(A, pay, stride, __shfl_sync(0xffffffffu, S.mine, 0));
-            if (S.mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, S.mine);
+            if (!A.have) offsets_from<CAT_ANY>(A, pay, stride, __shfl_sync(0xffffffffu, S.mine, 0));
+            if (S.mine >= 0) pair32<STRAT, KT, CAT_ANY>(A, C, Q, pay, stride, S.mine);
             if (fill == 32 && ++nb == CHUNK) {
-                A.flush(C, need_grad);
+                A.flush<CAT_ANY>(C);
                 nb = 0;
             }
         };
@@ -464,7 +507,7 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
             while (next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) deal(S, lane, lo, hi, proc);
         }
         if (S.fill > 0) proc(S.fill);
-        reduce_finalize32(A, C, need_grad, qi, lane);
+        reduce_finalize32<CAT_ANY>(A, C, qi, lane);
     }
 }
 
@@ -474,7 +517,7 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
 // fused kernel does, so both produce the same bits.  Within a chunk, lane l finds the run
 // holding its leaf by a binary search over the inclusive prefix sums of the run lengths
 // held one per lane.
-template <int STRAT, int KT>
+template <int STRAT, int KT, int CAT>
 __global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
                                                   RunPool P, int64_t m, const uint32_t *__restrict__ ql,
                                                   const uint32_t *__restrict__ order, const double *__restrict__ qx,
@@ -483,7 +526,6 @@ __global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, co
 {
     const int lane = threadIdx.x & 31;
     const float sig = ldexp_norm3(KT);
-    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
     for (;;) {
         int64_t t = next_query(counter, lane);
         if (t >= m) break;
@@ -493,31 +535,31 @@ __global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, co
         const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
         Query32 Q;
         Acc32 A;
-        setup32<STRAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride);
+        setup32<STRAT, CAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride);
         int nb = 0;   // full batches since the last flush (warp-uniform)
         int64_t mine = -1;
         auto first = [&](int64_t b0) {
-            if (!A.have) offsets_from(A, pay, stride, b0);
+            if (!A.have) offsets_from<CAT>(A, pay, stride, b0);
         };
         auto one = [&](int64_t b) {
-            pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, b);
+            pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, b);
             if (++nb == CHUNK) {
-                A.flush(C, need_grad);
+                A.flush<CAT>(C);
                 nb = 0;
             }
         };
         auto two = [&](int64_t m1) {   // flush boundary after the second batch (nb is even here)
-            pair32x2<STRAT, KT>(A, C, need_grad, Q, pay, stride, m1, m1 + 32);
+            pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
             nb += 2;
             if (nb == CHUNK) {
-                A.flush(C, need_grad);
+                A.flush<CAT>(C);
                 nb = 0;
             }
         };
         auto cantwo = [&]() { return (nb & 1) == 0; };
         deal_runs(P, j, lane, first, one, two, cantwo, mine);
-        if (mine >= 0) pair32<STRAT, KT>(A, C, need_grad, Q, pay, stride, mine);
-        reduce_finalize32(A, C, need_grad, qi, lane);
+        if (mine >= 0) pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, mine);
+        reduce_finalize32<CAT>(A, C, qi, lane);
     }
 }
 
@@ -577,14 +619,27 @@ cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C,
     return cudaGetLastError();
 }
 
-template <int STRAT, int KT>
+template <int STRAT, int KT, int CAT>
 static void launch_pairs_one(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride,
                              const RunPool &P, int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
                              const double *qy, const double *qz, unsigned long long *ctr)
 {
     const int bs = 128;
-    k_pairs32w<STRAT, KT><<<persistent_grid((const void *)k_pairs32w<STRAT, KT>, bs), bs, 0, H->stream>>>(
+    k_pairs32w<STRAT, KT, CAT><<<persistent_grid((const void *)k_pairs32w<STRAT, KT, CAT>, bs), bs, 0, H->stream>>>(
         T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr);
+}
+
+template <int STRAT, int KT>
+static void launch_pairs_cat(Handle *H, const DevTree &T, const DevCatalog &C, const float4 *pay, int stride,
+                             const RunPool &P, int64_t m, const uint32_t *ql, const uint32_t *order, const double *qx,
+                             const double *qy, const double *qz, unsigned long long *ctr)
+{
+    switch (catalog_shape(C)) {
+    case CAT_GDC4: launch_pairs_one<STRAT, KT, CAT_GDC4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case CAT_C4: launch_pairs_one<STRAT, KT, CAT_C4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case CAT_S1: launch_pairs_one<STRAT, KT, CAT_S1>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    default: launch_pairs_one<STRAT, KT, CAT_ANY>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    }
 }
 
 template <int STRAT>
@@ -593,12 +648,12 @@ static void launch_pairs_kt(Handle *H, const DevTree &T, const DevCatalog &C, co
                             const double *qy, const double *qz, unsigned long long *ctr)
 {
     switch (T.kernel) {
-    case 0: launch_pairs_one<STRAT, 0>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
-    case 1: launch_pairs_one<STRAT, 1>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
-    case 2: launch_pairs_one<STRAT, 2>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
-    case 3: launch_pairs_one<STRAT, 3>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
-    case 4: launch_pairs_one<STRAT, 4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
-    default: launch_pairs_one<STRAT, 5>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 0: launch_pairs_cat<STRAT, 0>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 1: launch_pairs_cat<STRAT, 1>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 2: launch_pairs_cat<STRAT, 2>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 3: launch_pairs_cat<STRAT, 3>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case 4: launch_pairs_cat<STRAT, 4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    default: launch_pairs_cat<STRAT, 5>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     }
 }
 
