@@ -358,7 +358,7 @@ def main():
         kname = {"M4_spline": "M4", "C4_Wendland": "C4"}.get(config["kernel"], config["kernel"])
         pk = "k_pairs32w<itpSymmetric,%s> (+ k_pairs64w for light queries)" % kname if prec == pb.FP32C \
             else "k_pairs64w<itpSymmetric>"
-        kern = {"walk": ("k_nearest_list + k_walk_items<itpSymmetric>", ph[0] + ph[1]), "pairs": (pk, ph[2])}
+        kern = {"walk": ("k_nearest_list + k_item_filter + k_walk_list<itpSymmetric>", ph[0] + ph[1]), "pairs": (pk, ph[2])}
         per = {}
         for key, (name, ms) in kern.items():
             a = alg[key] / (ms / 1e3) / 1e9 if ms > 0 else None

@@ -222,6 +222,11 @@ static cudaError_t exclusive_scan_u32(Handle *H, const uint32_t *in, uint32_t *o
     return cudaGetLastError();
 }
 
+cudaError_t launch_exclusive_scan_u32(Handle *H, const uint32_t *in, uint32_t *out, int64_t m)
+{
+    return exclusive_scan_u32(H, in, out, m);
+}
+
 // ------------------------------------------------------------------------------------
 // stable LSD radix sort, 8-bit digits
 template <typename K>

@@ -27,7 +27,7 @@ pb::Handle::~Handle()
                    &right, &escape, &parent, &bmin64, &bmax64, &hmax64, &counters, &m_s, &rho_s, &col_ptrs,
                    &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux,
                    &pool_runs, &pool_next, &pool_ctr, &items, &wbnear, &qacc, &qflag, &cut, &defer_a, &defer_b,
-                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota, &mlp_w, &mlp_m, &mlp_v, &mlp_g, &mlp_norm,
+                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota, &wl_cnt, &wl_off, &wl_s, &wl_j, &wl_sa, &wl_ja, &mlp_w, &mlp_m, &mlp_v, &mlp_g, &mlp_norm,
                    &mlp_scr, &mlp_idx, &mlp_x, &mlp_y, &mlp_loss, &sched_feat, &sched_pred, &sched_ql, &sched_tmp};
     for (DBuf *b : all) b->release();
     for (auto &b : in_cols) b.release();
@@ -663,7 +663,8 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                 H.interp_launches += 4;
             }
             if (round == 0) ev_record(H, 5);
-            CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
+            if (mode == 0 || ns == 1) CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
+            else CK(launch_walk_list(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
             H.interp_launches++;
             uint32_t *order = nullptr;
             int64_t m_heavy = 0;

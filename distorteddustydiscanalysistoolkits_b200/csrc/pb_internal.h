@@ -72,6 +72,7 @@ struct Handle {
     DBuf col_ptrs;      // device array of sorted column pointers
 
     // run lists of the two-phase point path (walk kernel -> pair kernels)
+    DBuf wl_cnt, wl_off, wl_s, wl_j, wl_sa, wl_ja;   // (query, subtree) work list of the walk
     DBuf pool_runs, pool_next, pool_ctr, items, wbnear, qacc, qflag, cut, defer_a, defer_b, lpt_k, lpt_v, lpt_ka,
         lpt_va, iota;
     int walk_split = 64;   // target number of subtrees each query's walk is split into
@@ -110,6 +111,7 @@ cudaError_t sort_pairs_u64(Handle *H, uint64_t *keys, uint32_t *vals, uint64_t *
                            int bits);
 cudaError_t sort_pairs_u32(Handle *H, uint32_t *keys, uint32_t *vals, uint32_t *kalt, uint32_t *valt, int64_t n,
                            int bits);
+cudaError_t launch_exclusive_scan_u32(Handle *H, const uint32_t *in, uint32_t *out, int64_t m);
 cudaError_t launch_dedupe(Handle *H, uint64_t *codes, int64_t n);
 cudaError_t launch_gather(Handle *H, int64_t n, const double *x, const double *y, const double *z, const double *h,
                           const double *m, const double *rho, const std::vector<const double *> &cols);
@@ -124,6 +126,9 @@ cudaError_t launch_nearest_list(Handle *H, const DevTree &T, int64_t m, const ui
                                 const double *qy, const double *qz, int *bnear);
 cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m, const uint32_t *ql,
                         const double *qx, const double *qy, const double *qz, unsigned long long *counter);
+cudaError_t launch_walk_list(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m,
+                             const uint32_t *ql, const double *qx, const double *qy, const double *qz,
+                             unsigned long long *counter);
 cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order);
 cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned light_max, bool plain,
                                uint32_t **order, int64_t *m_heavy);

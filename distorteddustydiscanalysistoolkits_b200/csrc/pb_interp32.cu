@@ -12,7 +12,7 @@
 //   * every quantity enters as an offset A_b - A_hat (A_hat = the nearest particle's value,
 //     or the first accepted neighbour's for scatter, as a double-float) so that
 //     gradient/divergence/curl F - A B cancels as little as possible;
-//   * each lane sums its terms in plain FP32 over chunks of 4 full batches of 32 pairs (4 of
+//   * each lane sums its terms in plain FP32 over chunks of 8 full batches of 32 pairs (8 of
 //     its own pairs) and adds each chunk sum, converted exactly, to an FP64 accumulator.
 // The per-query arithmetic depends only on the query and the tree (chunks are counted over
 // the query's own accepted-neighbour sequence), never on the launch shape or schedule.
@@ -24,7 +24,7 @@ namespace pb {
 
 __device__ const float g_line_inorm32[6][PB_LINE_NTAB] = PB_LINE_INORM_INIT;
 
-constexpr int CHUNK = 4;
+constexpr int CHUNK = 8;
 static_assert(CHUNK % 2 == 0, "pairs of batches must not straddle a flush");
 
 // ---- kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) in FP32 ----

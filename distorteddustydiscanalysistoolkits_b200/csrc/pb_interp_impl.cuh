@@ -229,6 +229,22 @@ __device__ __forceinline__ int64_t next_accepted(const DevTree &T, Walk &w, doub
     }
 }
 
+// The walk's pruning decision for internal node `node` (box `nd`): FP32 box distance with
+// directed rounding against the node radius (query radius and/or K * hmax) with the 2^-20
+// margin.  Shared by the walk and by the subtree prefilter so both decide alike.
+template <int STRAT>
+__device__ __forceinline__ bool node_pruned(const DevTree &T, const NodeF &nd, int node, const QBox &q, float Kf,
+                                            float r2a_up)
+{
+    float r2n;
+    if (STRAT == GATHER) r2n = r2a_up;
+    else {
+        float rr = sq_up(Kf, __ldg(T.node_hmax + (node - 1)));
+        r2n = STRAT == SCATTER ? rr : fmaxf(r2a_up, rr);
+    }
+    return box_lower(q, nd) > __fmul_ru(r2n, MARGIN_UP);
+}
+
 // Warp-uniform form of the same walk for the warp-per-query kernels: returns the next
 // accepted item in DFS order, either a single leaf (lo == hi) or the whole contiguous leaf
 // range of a subtree that lies inside the query radius.
@@ -260,13 +276,7 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
             continue;
         }
         NodeF nd = load_node(T.node + (node - 1));
-        float r2n;
-        if (STRAT == GATHER) r2n = r2a_up;
-        else {
-            float rr = sq_up(Kf, __ldg(T.node_hmax + (node - 1)));
-            r2n = STRAT == SCATTER ? rr : fmaxf(r2a_up, rr);
-        }
-        if (box_lower(q, nd) > __fmul_ru(r2n, MARGIN_UP)) { w.node = nd.escape; continue; }
+        if (node_pruned<STRAT>(T, nd, node, q, Kf, r2a_up)) { w.node = nd.escape; continue; }
         if (STRAT != SCATTER && box_upper(q, nd) <= bulk_lim) {
             int2 rg = __ldg(T.range + (node - 1));
             lo = rg.x;

@@ -124,6 +124,53 @@ struct RunWriter {
     __device__ __forceinline__ bool close(const RunPool &P) { return olo < 0 || store(P); }
 };
 
+// One (query, subtree) item: walk subtree s for the j-th listed query and write its runs.
+template <int STRAT>
+__device__ __forceinline__ void walk_item(const DevTree &T, const RunPool &P, int64_t j, int s,
+                                          const uint32_t *__restrict__ ql, const double *__restrict__ qx,
+                                          const double *__restrict__ qy, const double *__restrict__ qz, double K)
+{
+    const uint32_t qi = __ldg(ql + j);
+    bool ok = P.count_only || (*(volatile unsigned long long *)P.used < P.cap &&
+                               *(volatile int *)(P.qflag + j) == 0);   // pool exhausted or query deferred
+    RunWriter R;
+    if (ok) {
+        const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        double ha = 0.0;
+        if (STRAT != SCATTER) {
+            const int b = P.bnear[j];
+            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
+        }
+        const double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
+        if (T.root == 0) {
+            double4 L;
+            double d2;
+            if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2)) ok = R.emit(P, 0, 0);
+        } else {
+            const int2 c = __ldg(P.cut + s);
+            Walk w{c.x, 1, 0, 0, 4 * T.n + 64, c.y};
+            int64_t lo, hi;
+            while (ok && next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) ok = R.emit(P, lo, hi);
+        }
+        if (ok) ok = R.close(P);
+    }
+    const int64_t it = j * P.ns + s;
+    if (P.count_only) {
+        if (R.nacc > 0) atomicAdd(P.qacc + j, (unsigned)R.nacc);
+        return;
+    }
+    if (!ok) {
+        P.items[it] = make_int2(RUN_DEFERRED, 0);
+        if (atomicExch(P.qflag + j, 1) == 0) {
+            unsigned d = atomicAdd(P.n_deferred, 1u);
+            P.deferred[d] = qi;
+        }
+        return;
+    }
+    P.items[it] = make_int2(R.first, R.nruns);
+    if (R.nacc > 0) atomicAdd(P.qacc + j, (unsigned)R.nacc);
+}
+
 // warp items: (block of 32 list positions, subtree), query blocks outermost
 template <int STRAT>
 __global__ void __launch_bounds__(128) k_walk_items(DevTree T, RunPool P, int64_t m, const uint32_t *__restrict__ ql,
@@ -142,45 +189,70 @@ __global__ void __launch_bounds__(128) k_walk_items(DevTree T, RunPool P, int64_
         const int64_t j = (int64_t)(wi / ns) * 32 + lane;
         const int s = (int)(wi % ns);
         if (j >= m) continue;
+        walk_item<STRAT>(T, P, j, s, ql, qx, qy, qz, K);
+    }
+}
+
+// Subtree prefilter: an item whose subtree root the walk would prune at its first step gets
+// an empty record here and no walk; the others are counted (cnt[j]) and, with emit, listed
+// as (subtree, query) pairs at off[j].  The root test is the walk's own (node_pruned).
+template <int STRAT, bool EMIT>
+__global__ void __launch_bounds__(128) k_item_filter(DevTree T, RunPool P, int64_t m, const uint32_t *__restrict__ ql,
+                                                     const double *__restrict__ qx, const double *__restrict__ qy,
+                                                     const double *__restrict__ qz, uint32_t *cnt,
+                                                     const uint32_t *__restrict__ off, uint32_t *ws, uint32_t *wj)
+{
+    const double K = kernel_valid(T.kernel);
+    const float Kf = (float)K;
+    const int ns = P.ns;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t qi = __ldg(ql + j);
-        bool ok = P.count_only || (*(volatile unsigned long long *)P.used < P.cap &&
-                                   *(volatile int *)(P.qflag + j) == 0);   // pool exhausted or query deferred
-        RunWriter R;
-        if (ok) {
-            const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
-            double ha = 0.0;
-            if (STRAT != SCATTER) {
-                const int b = P.bnear[j];
-                ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
-            }
-            const double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
-            if (T.root == 0) {
-                double4 L;
-                double d2;
-                if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2)) ok = R.emit(P, 0, 0);
-            } else {
-                const int2 c = __ldg(P.cut + s);
-                Walk w{c.x, 1, 0, 0, 4 * T.n + 64, c.y};
-                int64_t lo, hi;
-                while (ok && next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) ok = R.emit(P, lo, hi);
-            }
-            if (ok) ok = R.close(P);
+        const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+        double ha = 0.0;
+        if (STRAT != SCATTER) {
+            const int b = P.bnear[j];
+            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
         }
-        const int64_t it = j * ns + s;
-        if (P.count_only) {
-            if (R.nacc > 0) atomicAdd(P.qacc + j, (unsigned)R.nacc);
-            continue;
-        }
-        if (!ok) {
-            P.items[it] = make_int2(RUN_DEFERRED, 0);
-            if (atomicExch(P.qflag + j, 1) == 0) {
-                unsigned d = atomicAdd(P.n_deferred, 1u);
-                P.deferred[d] = qi;
+        const double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
+        const QBox q = make_qbox(px, py, pz);
+        const float r2a_up = __double2float_ru(r2a);
+        uint32_t k = 0, base = EMIT ? off[j] : 0;
+        for (int s = 0; s < ns; ++s) {
+            const int node = __ldg(&P.cut[s].x);
+            bool walk = true;
+            if (T.root != 0 && node < T.n) walk = !node_pruned<STRAT>(T, load_node(T.node + (node - 1)), node, q, Kf, r2a_up);
+            if (walk) {
+                if (EMIT) {
+                    ws[base + k] = (uint32_t)s;
+                    wj[base + k] = (uint32_t)j;
+                }
+                ++k;
+            } else if (!EMIT) {
+                P.items[j * ns + s] = make_int2(-1, 0);
             }
-            continue;
         }
-        P.items[it] = make_int2(R.first, R.nruns);
-        if (R.nacc > 0) atomicAdd(P.qacc + j, (unsigned)R.nacc);
+        if (!EMIT) cnt[j] = k;
+    }
+}
+
+// walk over a (subtree, query) work list grouped by subtree: the lanes of a warp walk the same
+// subtree for neighbouring queries
+template <int STRAT>
+__global__ void __launch_bounds__(128) k_walk_list(DevTree T, RunPool P, int64_t nlist, const uint32_t *__restrict__ ws,
+                                                   const uint32_t *__restrict__ wj, const uint32_t *__restrict__ ql,
+                                                   const double *__restrict__ qx, const double *__restrict__ qy,
+                                                   const double *__restrict__ qz, unsigned long long *counter)
+{
+    const int lane = threadIdx.x & 31;
+    const double K = kernel_valid(T.kernel);
+    for (;;) {
+        unsigned long long wi = 0;
+        if (lane == 0) wi = atomicAdd(counter, 1ULL);
+        wi = __shfl_sync(0xffffffffu, wi, 0);
+        const int64_t k = (int64_t)wi * 32 + lane;
+        if ((int64_t)wi * 32 >= nlist) break;
+        if (k >= nlist) continue;
+        walk_item<STRAT>(T, P, (int64_t)__ldg(wj + k), (int)__ldg(ws + k), ql, qx, qy, qz, K);
     }
 }
 
@@ -287,6 +359,56 @@ cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool
     }
     H->launches += 1;
     return cudaGetLastError();
+}
+
+template <int STRAT>
+static cudaError_t walk_list_strat(Handle *H, const DevTree &T, const RunPool &P, int64_t m, const uint32_t *ql,
+                                   const double *qx, const double *qy, const double *qz, unsigned long long *counter)
+{
+    cudaError_t e;
+    if ((e = H->wl_cnt.reserve(sizeof(uint32_t) * (m + 1)))) return e;
+    if ((e = H->wl_off.reserve(sizeof(uint32_t) * (m + 1)))) return e;
+    uint32_t *cnt = H->wl_cnt.as<uint32_t>(), *off = H->wl_off.as<uint32_t>();
+    k_item_filter<STRAT, false><<<grid_for(m, 128, 1 << 30), 128, 0, H->stream>>>(T, P, m, ql, qx, qy, qz, cnt,
+                                                                                 nullptr, nullptr, nullptr);
+    if ((e = launch_exclusive_scan_u32(H, cnt, off, m))) return e;
+    uint32_t last[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(&last[0], off + (m - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, H->stream))) return e;
+    if ((e = cudaMemcpyAsync(&last[1], cnt + (m - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, H->stream))) return e;
+    if ((e = cudaStreamSynchronize(H->stream))) return e;
+    const int64_t nlist = (int64_t)last[0] + last[1];
+    H->launches += 1;
+    if (nlist == 0) return cudaSuccess;
+    if ((e = H->wl_s.reserve(sizeof(uint32_t) * nlist))) return e;
+    if ((e = H->wl_j.reserve(sizeof(uint32_t) * nlist))) return e;
+    if ((e = H->wl_sa.reserve(sizeof(uint32_t) * nlist))) return e;
+    if ((e = H->wl_ja.reserve(sizeof(uint32_t) * nlist))) return e;
+    uint32_t *ws = H->wl_s.as<uint32_t>(), *wj = H->wl_j.as<uint32_t>();
+    k_item_filter<STRAT, true><<<grid_for(m, 128, 1 << 30), 128, 0, H->stream>>>(T, P, m, ql, qx, qy, qz, nullptr,
+                                                                                off, ws, wj);
+    H->launches += 1;
+    int bits = 1;
+    while ((1 << bits) < P.ns) ++bits;
+    if ((e = sort_pairs_u32(H, ws, wj, H->wl_sa.as<uint32_t>(), H->wl_ja.as<uint32_t>(), nlist, bits))) return e;
+    if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), H->stream))) return e;
+    const int bs = 128;
+    k_walk_list<STRAT><<<persistent_blocks((const void *)k_walk_list<STRAT>, bs), bs, 0, H->stream>>>(
+        T, P, nlist, ws, wj, ql, qx, qy, qz, counter);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
+// the walk of a slice through the prefiltered (subtree, query) work list
+cudaError_t launch_walk_list(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m,
+                             const uint32_t *ql, const double *qx, const double *qy, const double *qz,
+                             unsigned long long *counter)
+{
+    if (m <= 0) return cudaSuccess;
+    switch (strategy) {
+    case GATHER: return walk_list_strat<GATHER>(H, T, P, m, ql, qx, qy, qz, counter);
+    case SCATTER: return walk_list_strat<SCATTER>(H, T, P, m, ql, qx, qy, qz, counter);
+    default: return walk_list_strat<SYMMETRIC>(H, T, P, m, ql, qx, qy, qz, counter);
+    }
 }
 
 cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order)
