@@ -52,9 +52,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c5"],
-                    help="c2: warped disc, cylindrical grid, L=11 (the headline); c5: clumped 16M disc, "
-                         "C4 Wendland, rho + curl v on a 256^3 Cartesian grid")
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: warped disc, cylindrical grid, L=11 (the headline); c3: two-species 8M disc, "
+                         "face-on column density + column-averaged vz image (line integrals, itpScatter); "
+                         "c5: clumped 16M disc, C4 Wendland, rho + curl v on a 256^3 Cartesian grid")
     ap.add_argument("--schedule", default="learned", choices=["plain", "tuned", "learned"],
                     help="query schedule of the FP32C path (outputs are identical)")
     ap.add_argument("--no-schedules", action="store_true", help="skip the plain/tuned/learned comparison")
@@ -233,6 +234,71 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_lines(args, rank, world):
+    """C3: line-integrated column density and column-averaged v_z of a 6M gas + 2M dust disc
+    (tilt 30 deg) on a face-on npix^2 image, both species per step; device-resident inputs."""
+    import ctypes
+    import torch
+    import distorteddustydiscanalysistoolkits_b200 as pb
+    from distorteddustydiscanalysistoolkits_b200 import _lib, synthetic
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ng, nd = (args.particles or 6291456), (args.particles or 6291456) // 3
+    npix = int(args.grid or 2048)
+    gas, dust = synthetic.dusty_disc(ng, nd, seed=3 + rank, tilt_deg=30.0)
+    lines = synthetic.face_on_lines(gas, npix=npix)
+    nl = len(lines)
+    prec = _lib.PB_FP32C if args.precision == "fp32c" else _lib.PB_FP64
+    be = pb.CUDAComputeBackend(int(os.environ.get("LOCAL_RANK", "0")))
+    H = be.handle
+    H.set_option("timing", 1)
+    H.set_stream(torch.cuda.current_stream().cuda_stream)
+    cat = pb.InterpolationCatalog(("rho", "vz"), scalars=("rho", "vz"))
+    o = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in lines.origin]
+    d = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in lines.direction]
+    species = []
+    for sp in (gas, dust):
+        dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in sp.items()}
+        inp = pb.InterpolationInput(dev["x"], dev["y"], dev["z"], dev["m"], dev["h"], dev["rho"],
+                                    (dev["rho"], dev["vz"]), smoothed_kernel=pb.M4_spline)
+        outs = [torch.empty(nl, dtype=torch.float64, device="cuda") for _ in range(cat.L)]
+        species.append((dev, inp, inp._c_struct(), outs, (ctypes.c_void_p * cat.L)(*[x.data_ptr() for x in outs])))
+    ccat = cat._c_struct()
+
+    def step():
+        b = i = 0.0
+        for dev, inp, cin, outs, optrs in species:
+            rc = H.lib.pb_line_samples_interpolation(H.h, ctypes.byref(cin), ctypes.byref(ccat), nl, o[0].data_ptr(),
+                                                     o[1].data_ptr(), o[2].data_ptr(), d[0].data_ptr(),
+                                                     d[1].data_ptr(), d[2].data_ptr(), pb.itpScatter.code, prec,
+                                                     optrs, 0)
+            H.check(rc, "pb_line_samples_interpolation")
+            tb, ti, _ = H.timings()
+            b += tb
+            i += ti
+        return b, i
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    res = [step() for _ in range(args.steps)]
+    build_ms = float(np.mean([r[0] for r in res]))
+    interp_ms = float(np.mean([r[1] for r in res]))
+    line = {"metric": "line samples/s (both species)", "value": 2 * nl / (interp_ms / 1e3), "unit": "lines/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": build_ms + interp_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32c" else "f64", "data": "synthetic (seeded two-species disc)",
+            "config": {"workload": "dusty disc %d gas + %d dust (M4, tilt 30 deg), face-on %d^2 image, itpScatter, "
+                                   "column rho + column-averaged vz per species" % (ng, nd, npix),
+                       "precision": args.precision},
+            "build_ms": build_ms, "interp_ms": interp_ms}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                f.write(json.dumps(line) + "\n")
+    return 0
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -240,6 +306,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.config == "c3":
+        return run_lines(args, rank, world)
 
     import torch
     import distorteddustydiscanalysistoolkits_b200 as pb
