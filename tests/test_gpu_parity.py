@@ -288,3 +288,19 @@ def test_traversal_stats_match_oracle(backend, strategy):
     cat = pb.InterpolationCatalog(COLS, scalars=("rho",))
     _, exp = _oracle(p).interp_points(cat.oracle_dict(), *flat.coor, strategy=strategy, stats=True)
     assert np.array_equal(st, exp)
+
+
+def test_c1_full_size_fp64_bitexact(backend):
+    """The CPU-runnable configuration at full size: 131,072-particle disc (seed 1), M4, scalar rho
+    (no Shepard normalisation for :rho) on a 64^3 Cartesian grid over the disc, FP64,
+    itpSymmetric -- every one of the 262,144 values equals the oracle's bit for bit."""
+    p = synthetic.disc(131072, seed=1)
+    flat = pb.flatten(pb.Cartesian, synthetic.cartesian_box_grid(p, n=64))
+    cat = pb.InterpolationCatalog(("rho",), scalars=("rho",))
+    assert cat.scalar_snormalization == (False,)
+    out = pb.PointSamples_interpolation(backend, flat, _input(p, cols=("rho",)), cat, pb.itpSymmetric,
+                                        precision=pb.FP64)
+    exp = _oracle(p, cols=("rho",)).interp_points(cat.oracle_dict(), *flat.coor, strategy="itpSymmetric")
+    got = np.stack([g.grid for g in out.grids])
+    assert np.isfinite(exp).sum() > 0.5 * exp.size
+    _assert_same(got, exp)
