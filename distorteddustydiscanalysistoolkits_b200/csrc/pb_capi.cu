@@ -27,7 +27,7 @@ pb::Handle::~Handle()
                    &right, &escape, &parent, &bmin64, &bmax64, &hmax64, &counters, &m_s, &rho_s, &col_ptrs,
                    &q_x, &q_y, &q_z, &q_keys, &q_keys_alt, &q_perm, &q_perm_alt, &q_out, &q_aux,
                    &pool_runs, &pool_next, &pool_ctr, &items, &wbnear, &qacc, &qflag, &cut, &defer_a, &defer_b,
-                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota, &wl_cnt, &wl_off, &wl_s, &wl_j, &wl_sa, &wl_ja, &mlp_w, &mlp_m, &mlp_v, &mlp_g, &mlp_norm,
+                   &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota, &grid_ax, &grid_out, &wl_cnt, &wl_off, &wl_s, &wl_j, &wl_sa, &wl_ja, &mlp_w, &mlp_m, &mlp_v, &mlp_g, &mlp_norm,
                    &mlp_scr, &mlp_idx, &mlp_x, &mlp_y, &mlp_loss, &sched_feat, &sched_pred, &sched_ql, &sched_tmp};
     for (DBuf *b : all) b->release();
     for (auto &b : in_cols) b.release();
@@ -1107,6 +1107,39 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
 }
 
 int64_t pb_launch_count(const pb_handle *h) { return h ? h->H.launches : 0; }
+
+int32_t pb_grid_points(pb_handle *h, int32_t coord, const double *a0, int64_t n0, const double *a1, int64_t n1,
+                       const double *a2, int64_t n2, double *x, double *y, double *z)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (coord != 0 && coord != 2 && coord != 3)
+        return fail(H, PB_ERR_INVALID, "coordinate system must be 0 (Cartesian), 2 (cylindrical) or 3 (spherical)");
+    if (!a0 || !a1 || !a2 || !x || !y || !z || n0 < 1 || n1 < 1 || n2 < 1)
+        return fail(H, PB_ERR_INVALID, "grid axes / outputs: bad arguments");
+    const int64_t n = n0 * n1 * n2;
+    CK(cudaSetDevice(H.device));
+    CK(H.grid_ax.reserve(sizeof(double) * (n0 + n1 + n2)));
+    double *ax = H.grid_ax.as<double>();
+    CK(cudaMemcpyAsync(ax, a0, sizeof(double) * n0, cudaMemcpyDefault, H.stream));
+    CK(cudaMemcpyAsync(ax + n0, a1, sizeof(double) * n1, cudaMemcpyDefault, H.stream));
+    CK(cudaMemcpyAsync(ax + n0 + n1, a2, sizeof(double) * n2, cudaMemcpyDefault, H.stream));
+    double *outs[3] = {x, y, z};
+    double *dst[3];
+    const bool dev = is_device_ptr(x) && is_device_ptr(y) && is_device_ptr(z);
+    if (!dev) {
+        CK(H.grid_out.reserve(sizeof(double) * 3 * n));
+        for (int d = 0; d < 3; ++d) dst[d] = H.grid_out.as<double>() + d * n;
+    } else {
+        for (int d = 0; d < 3; ++d) dst[d] = outs[d];
+    }
+    CK(launch_grid_points(&H, coord, ax, n0, ax + n0, n1, ax + n0 + n1, n2, dst[0], dst[1], dst[2]));
+    if (!dev)
+        for (int d = 0; d < 3; ++d)
+            CK(cudaMemcpyAsync(outs[d], dst[d], sizeof(double) * n, cudaMemcpyDeviceToHost, H.stream));
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
 
 // ---- learned work prediction ----
 namespace {

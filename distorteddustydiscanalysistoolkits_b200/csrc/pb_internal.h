@@ -72,6 +72,7 @@ struct Handle {
     DBuf col_ptrs;      // device array of sorted column pointers
 
     // run lists of the two-phase point path (walk kernel -> pair kernels)
+    DBuf grid_ax, grid_out;   // axes / points of pb_grid_points
     DBuf wl_cnt, wl_off, wl_s, wl_j, wl_sa, wl_ja;   // (query, subtree) work list of the walk
     DBuf pool_runs, pool_next, pool_ctr, items, wbnear, qacc, qflag, cut, defer_a, defer_b, lpt_k, lpt_v, lpt_ka,
         lpt_va, iota;
@@ -171,6 +172,8 @@ cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double
 cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
                          const double *qz, const double *radius, const int64_t *offsets, int64_t *counts,
                          int64_t *pool, int64_t *nearest);
+cudaError_t launch_grid_points(Handle *H, int coord, const double *a0, int64_t n0, const double *a1, int64_t n1,
+                               const double *a2, int64_t n2, double *x, double *y, double *z);
 cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, const double *qx, const double *qy,
                          const double *qz, int64_t *stats);
 

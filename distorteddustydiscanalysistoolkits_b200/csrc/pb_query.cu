@@ -175,4 +175,40 @@ cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *
     return cudaGetLastError();
 }
 
+// Sample points of a structured grid, generated on the device (coordinate_grid + flatten,
+// StructuredGrid.jl:126-204, transform.jl:53-66): column-major linear order, the first axis
+// fastest; coord 0 Cartesian (a0, a1, a2), 2 cylindrical (s cos phi, s sin phi, z), 3 spherical
+// (r sin(theta) cos(phi), r sin(theta) sin(phi), r cos(theta)) with the host's operation order.
+__global__ void k_grid_points(int coord, const double *__restrict__ a0, int64_t n0, const double *__restrict__ a1,
+                              int64_t n1, const double *__restrict__ a2, int64_t n2, double *x, double *y, double *z)
+{
+    const int64_t n = n0 * n1 * n2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i0 = i % n0, i1 = (i / n0) % n1, i2 = i / (n0 * n1);
+        const double u = a0[i0], v = a1[i1], w = a2[i2];
+        if (coord == 2) {
+            x[i] = __dmul_rn(u, cos(v));
+            y[i] = __dmul_rn(u, sin(v));
+            z[i] = w;
+        } else if (coord == 3) {
+            const double st = sin(w);
+            x[i] = __dmul_rn(__dmul_rn(u, st), cos(v));
+            y[i] = __dmul_rn(__dmul_rn(u, st), sin(v));
+            z[i] = __dmul_rn(u, cos(w));
+        } else {
+            x[i] = u;
+            y[i] = v;
+            z[i] = w;
+        }
+    }
+}
+
+cudaError_t launch_grid_points(Handle *H, int coord, const double *a0, int64_t n0, const double *a1, int64_t n1,
+                               const double *a2, int64_t n2, double *x, double *y, double *z)
+{
+    k_grid_points<<<grid_for(n0 * n1 * n2, 256), 256, 0, H->stream>>>(coord, a0, n0, a1, n1, a2, n2, x, y, z);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
 }  // namespace pb

@@ -338,11 +338,47 @@ def LineSamples_interpolation(backend, grid_template, input, catalog, itp_strate
     return GridBundle([LineSamples(v, o, d) for v in outs], catalog.ordered_names)
 
 
+_COORD_CODE = {"Cartesian": 0, "Cylindrical": 2, "Spherical": 3}
+
+
+def grid_points_device(backend, coord, grid_template):
+    """The flattened sample points of a 3D StructuredGrid, generated on the backend's device
+    (pb_grid_points): three CUDA float64 tensors in column-major order (first axis fastest)."""
+    import torch
+    code = _COORD_CODE.get(coord.__name__)
+    if code is None or len(grid_template.axes) != 3:
+        raise ArgumentError("device grid points need a 3D Cartesian, Cylindrical or Spherical grid")
+    axes = [np.ascontiguousarray(a, np.float64) for a in grid_template.axes]
+    n = int(np.prod([len(a) for a in axes]))
+    out = [torch.empty(n, dtype=torch.float64, device="cuda:%d" % backend.device) for _ in range(3)]
+    H = backend.handle
+    H.check(H.lib.pb_grid_points(H.h, code, ptr(axes[0]), len(axes[0]), ptr(axes[1]), len(axes[1]), ptr(axes[2]),
+                                 len(axes[2]), out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr()), "grid_points")
+    return out
+
+
 def StructuredGrid_interpolation(backend, coord, grid_template, input, catalog, itp_strategy=itpSymmetric,
-                                 precision=FP64):
-    """flatten -> PointSamples_interpolation -> restore_struct (StructuredGrid_interpolation.jl:46-64)."""
+                                 precision=FP64, points_on_device=False):
+    """flatten -> PointSamples_interpolation -> restore_struct (StructuredGrid_interpolation.jl:46-64).
+
+    With ``points_on_device`` the sample points are generated on the device (grid_points_device)
+    and never copied from the host; the outputs are reshaped directly (the generated points
+    follow the axes by construction)."""
     if not isinstance(grid_template, StructuredGrid):
         raise ArgumentError("grid_template must be a StructuredGrid")
+    if points_on_device:
+        q = grid_points_device(backend, coord, grid_template)
+        H = backend.handle
+        n = len(q[0])
+        outs = _out_arrays(n, catalog.L)
+        cin, ccat = input._c_struct(), catalog._c_struct()
+        rc = H.lib.pb_point_samples_interpolation(H.h, ctypes.byref(cin), ctypes.byref(ccat), n, q[0].data_ptr(),
+                                                  q[1].data_ptr(), q[2].data_ptr(), _strategy(itp_strategy),
+                                                  _precision(precision), _ptr_array(outs), _lib.PB_PERMUTE_CALLER)
+        H.check(rc, "StructuredGrid_interpolation")
+        size = tuple(len(a) for a in grid_template.axes)
+        grids = [StructuredGrid(np.asarray(o).reshape(size, order="F"), grid_template.axes, size) for o in outs]
+        return GridBundle(grids, catalog.ordered_names)
     flat = flatten(coord, grid_template)
     bundle = PointSamples_interpolation(backend, flat, input, catalog, itp_strategy, precision)
     grids = [restore_struct(coord, g, grid_template.axes) for g in bundle.grids]

@@ -172,6 +172,15 @@ int32_t pb_morton_sort_noalloc(const double *x, const double *y, const double *z
 int64_t pb_launch_count(const pb_handle *h);
 int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms, int64_t *interp_launches);
 
+/* Sample points of a structured grid generated on the device: coordinate_grid + flatten
+   (Partia.jl/src/julia/Grids/grids/StructuredGrid.jl:126-204, grids/transform.jl:53-66),
+   column-major (first axis fastest).  coord: 0 Cartesian (axes x, y, z), 2 cylindrical
+   (s, phi, z), 3 spherical (r, phi, theta).  Axes may be host or device arrays; when x, y, z
+   are device arrays the points never leave the device (no host-to-device copy of sample
+   coordinates).  Trigonometric values are the device's libm, within 2 ulp of the host's. */
+int32_t pb_grid_points(pb_handle *h, int32_t coord, const double *a0, int64_t n0, const double *a1, int64_t n1,
+                       const double *a2, int64_t n2, double *x, double *y, double *z);
+
 /* Learned work prediction for the FP32-compensated point schedule (no counterpart in the
    reference; the reference runs queries in input order).  A 3-layer MLP of width 64 with
    BF16 weights and activations (PB_SCHED_FEATURES inputs, PB_SCHED_PARAMS parameters laid out
