@@ -288,6 +288,59 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
     }
 }
 
+// Flat form of the same walk for one thread, over the subtree entered at `start` and left at
+// `stop`: one node step per loop iteration, and every accepted item (a single leaf, or the
+// whole leaf range of a subtree inside the query radius) passed to emit(lo, hi) in DFS order.
+// The decisions are next_item's, step for step; a warp running this loop reconverges once
+// per node step instead of once per accepted item.  Returns false if emit refused an item.
+template <int STRAT, typename EMIT>
+__device__ __forceinline__ bool walk_subtree(const DevTree &T, int start, int stop, double px, double py, double pz,
+                                             double K, double r2a, EMIT &emit)
+{
+    const int64_t n = T.n;
+    const QBox q = make_qbox(px, py, pz);
+    const float Kf = (float)K;
+    const float r2a_up = __double2float_ru(r2a);
+    const float bulk_lim = __fmul_rd(__double2float_rd(r2a), MARGIN_DN);
+    const int64_t limit = 4 * n + 64;
+    int64_t guard = 0;
+    int node = start;
+    while (node != stop) {
+        if (++guard > limit) {
+            flag(T.status, ST_TRAVERSAL);
+            break;
+        }
+        int64_t lo = -1, hi = -1;
+        if (node >= n) {
+            const int64_t b = node - n;
+            const double4 L = ldg4(T.leaf + b);
+            node = __ldg(T.leaf_escape + b);
+            double r2;
+            if (STRAT == GATHER) r2 = r2a;
+            else {
+                const double r = __dmul_rn(K, L.w);
+                const double rr = __dmul_rn(r, r);
+                r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+            }
+            if (d2_point(px, py, pz, L) <= r2) lo = hi = b;
+        } else {
+            const NodeF nd = load_node(T.node + (node - 1));
+            if (node_pruned<STRAT>(T, nd, node, q, Kf, r2a_up)) {
+                node = nd.escape;
+            } else if (STRAT != SCATTER && box_upper(q, nd) <= bulk_lim) {
+                const int2 rg = __ldg(T.range + (node - 1));
+                lo = rg.x;
+                hi = rg.y;
+                node = nd.escape;
+            } else {
+                node = nd.left;
+            }
+        }
+        if (lo >= 0 && !emit(lo, hi)) return false;
+    }
+    return true;
+}
+
 // Slot filler shared by the warp-per-query kernels: accepted leaves, in DFS order, are
 // dealt to the 32 lanes (the k-th accepted leaf goes to lane k mod 32); PROC(fill) is
 // called whenever 32 slots are full and once more for the remainder.

@@ -148,9 +148,8 @@ __device__ __forceinline__ void walk_item(const DevTree &T, const RunPool &P, in
             if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2)) ok = R.emit(P, 0, 0);
         } else {
             const int2 c = __ldg(P.cut + s);
-            Walk w{c.x, 1, 0, 0, 4 * T.n + 64, c.y};
-            int64_t lo, hi;
-            while (ok && next_item<STRAT>(T, w, px, py, pz, K, r2a, lo, hi)) ok = R.emit(P, lo, hi);
+            auto emit = [&](int64_t lo, int64_t hi) { return R.emit(P, lo, hi); };
+            ok = walk_subtree<STRAT>(T, c.x, c.y, px, py, pz, K, r2a, emit);
         }
         if (ok) ok = R.close(P);
     }
