@@ -165,20 +165,24 @@ __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int s
     }
 }
 
-// FP64 accumulator of FP32 chunk sums: the conversion is exact and the FP64 additions carry
-// 29 more bits than the terms, so the chunk sums are the only FP32 rounding left
-struct DSum {
-    double d;
-    __device__ __forceinline__ void zero() { d = 0.0; }
-    __device__ __forceinline__ void add(float x) { d = __dadd_rn(d, (double)x); }
-    __device__ __forceinline__ double val() const { return d; }
-};
+// The 15 FP64 sums of a thread live in shared memory (slot k at sa[k * ACC_STRIDE]): the pair
+// loop touches them once every CHUNK batches, so they need not hold registers.  Slots: 0 S1,
+// 1-4 SA, 5-7 B, 8-10 F, 11 D, 12-14 curl.
+constexpr int ACC_STRIDE = 128;   // threads per block of the kernels that use Acc32
+constexpr int ACC_SLOTS = 15;
 
 struct Acc32 {
     float pS1, pSA[MAXU], pB[3], pF[MAXG][3], pD[MAXD], pC[MAXC][3];
-    DSum S1, SA[MAXU], B[3], F[MAXG][3], D[MAXD], Cc[MAXC][3];
     float hh[MAXU], hl[MAXU];
+    double *sa;
     bool have;
+
+    __device__ __forceinline__ void addk(int k, float x)
+    {
+        double &d = sa[k * ACC_STRIDE];
+        d = __dadd_rn(d, (double)x);
+    }
+    __device__ __forceinline__ double getk(int k) const { return sa[k * ACC_STRIDE]; }
 
     __device__ __forceinline__ void zero_partials()
     {
@@ -195,20 +199,14 @@ struct Acc32 {
         for (int j = 0; j < MAXC; ++j) pC[j][0] = pC[j][1] = pC[j][2] = 0.f;
     }
 
-    __device__ __forceinline__ void init()
+    __device__ __forceinline__ void init(double *slots)
     {
+        sa = slots;
         zero_partials();
-        S1.zero();
 #pragma unroll
-        for (int u = 0; u < MAXU; ++u) { SA[u].zero(); hh[u] = 0.f; hl[u] = 0.f; }
+        for (int k = 0; k < ACC_SLOTS; ++k) sa[k * ACC_STRIDE] = 0.0;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) B[d].zero();
-#pragma unroll
-        for (int j = 0; j < MAXG; ++j) { F[j][0].zero(); F[j][1].zero(); F[j][2].zero(); }
-#pragma unroll
-        for (int j = 0; j < MAXD; ++j) D[j].zero();
-#pragma unroll
-        for (int j = 0; j < MAXC; ++j) { Cc[j][0].zero(); Cc[j][1].zero(); Cc[j][2].zero(); }
+        for (int u = 0; u < MAXU; ++u) { hh[u] = 0.f; hl[u] = 0.f; }
         have = false;
     }
 
@@ -216,16 +214,16 @@ struct Acc32 {
     __device__ __forceinline__ void flush(const DevCatalog &C)
     {
         using S = CatShape<CAT>;
-        S1.add(pS1);
+        addk(0, pS1);
 #pragma unroll
         for (int u = 0; u < MAXU; ++u)
-            if (u < S::nu(C)) SA[u].add(pSA[u]);
+            if (u < S::nu(C)) addk(1 + u, pSA[u]);
         if (S::any(C)) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) B[d].add(pB[d]);
-            if (S::grad(C)) { F[0][0].add(pF[0][0]); F[0][1].add(pF[0][1]); F[0][2].add(pF[0][2]); }
-            if (S::div(C)) D[0].add(pD[0]);
-            if (S::curl(C)) { Cc[0][0].add(pC[0][0]); Cc[0][1].add(pC[0][1]); Cc[0][2].add(pC[0][2]); }
+            for (int d = 0; d < 3; ++d) addk(5 + d, pB[d]);
+            if (S::grad(C)) { addk(8, pF[0][0]); addk(9, pF[0][1]); addk(10, pF[0][2]); }
+            if (S::div(C)) addk(11, pD[0]);
+            if (S::curl(C)) { addk(12, pC[0][0]); addk(13, pC[0][1]); addk(14, pC[0][2]); }
         }
         zero_partials();
     }
@@ -409,7 +407,7 @@ __device__ __forceinline__ void finalize32w(const double *v, const Acc32 &A, con
 // pairs, and the quantity offsets (nearest particle, else the first accepted neighbour)
 template <int STRAT, int CAT>
 __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, double py, double pz, int64_t bnear,
-                                        Query32 &Q, Acc32 &A, const float4 *pay, int stride)
+                                        Query32 &Q, Acc32 &A, const float4 *pay, int stride, double *slots)
 {
     Q = Query32{};
     if (STRAT != SCATTER) {
@@ -422,7 +420,7 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
     Q.ph[0] = (float)px; Q.pl[0] = (float)(px - (double)Q.ph[0]);
     Q.ph[1] = (float)py; Q.pl[1] = (float)(py - (double)Q.ph[1]);
     Q.ph[2] = (float)pz; Q.pl[2] = (float)(pz - (double)Q.ph[2]);
-    A.init();
+    A.init(slots);
     if (bnear >= 0) {
         // quantities enter as offsets from the nearest particle's values, which are close
         // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
@@ -446,13 +444,8 @@ __device__ __forceinline__ void reduce_finalize32(Acc32 &A, const DevCatalog &C,
 {
     A.flush<CAT>(C);
     double v[15];
-    v[0] = A.S1.val();
 #pragma unroll
-    for (int u = 0; u < MAXU; ++u) v[1 + u] = A.SA[u].val();
-    v[5] = A.B[0].val(); v[6] = A.B[1].val(); v[7] = A.B[2].val();
-    v[8] = A.F[0][0].val(); v[9] = A.F[0][1].val(); v[10] = A.F[0][2].val();
-    v[11] = A.D[0].val();
-    v[12] = A.Cc[0][0].val(); v[13] = A.Cc[0][1].val(); v[14] = A.Cc[0][2].val();
+    for (int k = 0; k < ACC_SLOTS; ++k) v[k] = A.getk(k);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
@@ -470,6 +463,7 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
                                                    const uint32_t *__restrict__ perm, int64_t npts,
                                                    unsigned long long *counter)
 {
+    __shared__ double s_acc[ACC_SLOTS * ACC_STRIDE];   // FP64 sums, slot k of thread t at [k * 128 + t]
     const int lane = threadIdx.x & 31;
     const int64_t n = T.n;
     const double K = kernel_valid(KT);
@@ -486,7 +480,7 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         double ra = __dmul_rn(K, ha), r2a = __dmul_rn(ra, ra);
         Query32 Q;
         Acc32 A;
-        setup32<STRAT, CAT_ANY>(T, sig, px, py, pz, bnear, Q, A, pay, stride);
+        setup32<STRAT, CAT_ANY>(T, sig, px, py, pz, bnear, Q, A, pay, stride, s_acc + threadIdx.x);
         Slots S{0, -1};
         int nb = 0;   // full batches since the last flush (warp-uniform)
         auto proc = [&](int fill) {
@@ -518,12 +512,13 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
 // holding its leaf by a binary search over the inclusive prefix sums of the run lengths
 // held one per lane.
 template <int STRAT, int KT, int CAT>
-__global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
+__global__ void __launch_bounds__(128, 5) k_pairs32w(DevTree T, DevCatalog C, const float4 *__restrict__ pay, int stride,
                                                   RunPool P, int64_t m, const uint32_t *__restrict__ ql,
                                                   const uint32_t *__restrict__ order, const double *__restrict__ qx,
                                                   const double *__restrict__ qy, const double *__restrict__ qz,
                                                   unsigned long long *counter)
 {
+    __shared__ double s_acc[ACC_SLOTS * ACC_STRIDE];   // FP64 sums, slot k of thread t at [k * 128 + t]
     const int lane = threadIdx.x & 31;
     const float sig = ldexp_norm3(KT);
     for (;;) {
@@ -535,7 +530,8 @@ __global__ void __launch_bounds__(128, 4) k_pairs32w(DevTree T, DevCatalog C, co
         const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
         Query32 Q;
         Acc32 A;
-        setup32<STRAT, CAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride);
+        setup32<STRAT, CAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride,
+                            s_acc + threadIdx.x);
         int nb = 0;   // full batches since the last flush (warp-uniform)
         int64_t mine = -1;
         auto first = [&](int64_t b0) {
