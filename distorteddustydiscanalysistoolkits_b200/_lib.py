@@ -202,7 +202,7 @@ class Handle:
         return r.value, d.value, c.value
 
     def phase_times(self):
-        """Device ms of the first round's nearest search, walk and pair sums (option "timing")."""
+        """Device ms of the nearest search, walk and pair sums, summed over slices and rounds (option "timing")."""
         t = (ctypes.c_double * 3)()
         self.lib.pb_last_schedule(self.h, None, None, None, t)
         return tuple(t)

@@ -642,7 +642,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
             P.deferred = lists[round & 1];
             P.count_only = 0;
-            if (round == 0) ev_record(H, 4);
+            ev_record(H, 4);
             if (strategy != SCATTER || mode == 2) {
                 CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
                 H.interp_launches++;
@@ -662,14 +662,14 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                 ql = qn;
                 H.interp_launches += 4;
             }
-            if (round == 0) ev_record(H, 5);
+            ev_record(H, 5);
             if (mode == 0 || ns == 1) CK(launch_walk(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
             else CK(launch_walk_list(&H, T, strategy, P, m, ql, dx, dy, dz, ctr + 2));
             H.interp_launches++;
             uint32_t *order = nullptr;
             int64_t m_heavy = 0;
             CK(launch_split_order(&H, P, m, (unsigned)H.light_max, mode == 0, &order, &m_heavy));
-            if (round == 0) ev_record(H, 6);
+            ev_record(H, 6);
             if (m_heavy > 0)
                 for (const Launch &Lc : launches) {
                     DevCatalog C = dev_catalog(H, Lc, dev.data());
@@ -682,7 +682,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                     CK(launch_pairs_fp64(&H, T, C, strategy, P, m - m_heavy, ql, order + m_heavy, dx, dy, dz));
                     H.interp_launches++;
                 }
-            if (round == 0) ev_record(H, 7);
+            ev_record(H, 7);
             unsigned long long used_nd[2] = {0, 0};
             CK(cudaMemcpyAsync(used_nd, ctr, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, H.stream));
             CK(cudaStreamSynchronize(H.stream));
@@ -698,8 +698,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                     Snext = std::max<int64_t>(1024, Snext / 2);
                 }
             }
-            if (round == 0)
-                for (int k = 0; k < 3; ++k) H.t_phase_ms[k] += ev_ms(H, 4 + k, 5 + k);
+            for (int k = 0; k < 3; ++k) H.t_phase_ms[k] += ev_ms(H, 4 + k, 5 + k);   // every slice and round
             H.walk_rounds = std::max<int64_t>(H.walk_rounds, round + 1);
             if (nd == 0) break;
             H.deferred_total += nd;

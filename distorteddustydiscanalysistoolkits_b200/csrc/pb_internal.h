@@ -97,7 +97,7 @@ struct Handle {
     bool timing = false;
     cudaEvent_t ev[8] = {};
     float t_build_ms = 0.f, t_interp_ms = 0.f;
-    float t_phase_ms[3] = {0.f, 0.f, 0.f};   // first walk round: nearest search, walk (+ ordering), pairs
+    float t_phase_ms[3] = {0.f, 0.f, 0.f};   // nearest search, walk (+ ordering), pairs; all slices and rounds
     int64_t interp_launches = 0;
     int sort_queries = 1;
     int block_size = 128;

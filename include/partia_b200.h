@@ -207,8 +207,9 @@ int32_t pb_scheduler_train(pb_handle *h, const float *X, const float *y, int64_t
 /* Diagnostics of the last FP32-compensated point call (no counterpart in the reference):
    walk rounds taken, queries deferred because the accepted-run pool was full (they are walked
    again, or finished by the fused kernel), the pool size in chunks of 32 runs, and (with
-   option "timing") the device time in ms of the first round's phases in phase_ms[3]: nearest
-   search, walk (with the heaviest-first ordering), pair sums.  The pool follows
+   option "timing") the device time in ms of the phases, summed over slices and walk rounds,
+   in phase_ms[3]: nearest search (with the learned binning), walk (with the prefilter and the
+   pair ordering), pair sums.  The pool follows
    PB_RUN_POOL_MB (MiB) or PB_RUN_POOL_CHUNKS from the environment when set. */
 int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks,
                          double *phase_ms);
