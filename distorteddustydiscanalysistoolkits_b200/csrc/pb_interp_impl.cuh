@@ -1,14 +1,13 @@
-// pb_interp_impl.cuh -- fused nearest-h search + ball-query traversal + SPH kernel sums,
-// one thread per sample point, stackless left/escape DFS (LinearBVHTraversalMacros.jl:26-371).
+// pb_interp_impl.cuh -- the traversal building blocks shared by the interpolation units:
+// nearest-h search, the stackless left/escape DFS of the ball query
+// (LinearBVHTraversalMacros.jl:26-371) in its warp-uniform (next_item) and flat per-thread
+// (walk_subtree) forms, the dealing of a query's accepted runs to the lanes of a warp
+// (deal_runs), the FP64 accumulator of the reference's arithmetic and the line kernel.
 //
-// Included by two translation units:
-//   pb_interp64.cu (-fmad=false): Exact64 -- every per-pair term and the finalisation use the
-//       reference's FP64 expressions in the reference's order (general_interpolation.jl,
-//       accumulations/*.jl, kernel.jl), so the results equal the FP64 oracle bit for bit.
-//   pb_interp32.cu: Comp32 -- the same neighbour sets (FP64 distance tests), FP64 pair
-//       offsets, kernel values and per-pair terms in FP32, TwoSum-compensated sums, and an
-//       offset formulation A_b - A_hat for every quantity (A_hat = first accepted neighbour's
-//       value) so that the gradient/divergence/curl differences F - A*B do not cancel in FP32.
+// Included by pb_interp64.cu (-fmad=false; FP64 terms in the reference's expressions and
+// order, bit-exact with the FP64 oracle), pb_interp32.cu (FP32 per-pair terms with double-float
+// offsets, FP64 accumulation of FP32 chunk sums; the FP32 line kernel uses TwoSum) and
+// pb_walk.cu (the walk kernels).
 //
 // Accepted neighbours are visited in ascending sorted-leaf order (DFS preorder), exactly as
 // in the reference, so the per-query summation order does not depend on the launch shape.
