@@ -595,7 +595,9 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
     if (mode == 2 && !H.mlp_ready) return fail(H, PB_ERR_STATE, "learned schedule requested but no scheduler weights set");
     int ns = 1;
     CK(launch_cut(&H, T, mode == 0 ? 1 : H.walk_split, &ns));
-    const int64_t S = H.slice > 0 ? std::min<int64_t>(H.slice, npts) : npts;
+    // a slice holds at most 2^31 - 1 (query, subtree) items: the work-list offsets are 32-bit
+    const int64_t S_items = std::max<int64_t>(1024, (int64_t)0x7fffffff / std::max(ns, 1));
+    const int64_t S = std::min<int64_t>(std::min<int64_t>(H.slice > 0 ? H.slice : npts, npts), S_items);
     int rc = reserve_pool(H, S, ns);
     if (rc) return rc;
     const uint32_t *ql_all = mode == 0 ? nullptr : perm;
