@@ -449,15 +449,13 @@ def main():
     # accuracy of the FP32-compensated fields against the FP64 path (bit-exact to the oracle)
     accuracy = None
     if prec == pb.FP32C and not args.no_accuracy:
+        from distorteddustydiscanalysistoolkits_b200 import accuracy as acc_mod
         ref = pb.interpolate_points(lb, cat, q, pb.itpSymmetric, pb.FP64)
         got = pb.interpolate_points(lb, cat, q, pb.itpSymmetric, pb.FP32C)
-        accuracy = {}
-        for name, a, r in zip(cat.ordered_names, got, ref):
-            a, r = a.cpu().numpy(), r.cpu().numpy()
-            ok = ~np.isnan(r)
-            sc = np.max(np.abs(r[ok]))
-            err = np.abs(a[ok] - r[ok]) / sc
-            accuracy[name] = {"max_field_scaled": float(err.max()), "rms_field_scaled": float(np.sqrt(np.mean(err ** 2)))}
+        split = H.pair_split()
+        accuracy = acc_mod.field_errors([a.cpu().numpy() for a in got], [r.cpu().numpy() for r in ref],
+                                        cat.ordered_names)
+        accuracy["pair_split"] = dict(zip(("heavy_queries", "light_queries", "heavy_pairs", "light_pairs"), split))
 
     # end to end through the public API with pinned host buffers
     e2e = None

@@ -13,7 +13,8 @@ from .interpolation import (C2_Wendland, C4_Wendland, C6_Wendland, CUDAComputeBa
                             M5_spline, M6_spline, LineSamples_interpolation, PointSamples_interpolation,
                             StructuredGrid_interpolation, build_input, interpolate_lines, interpolate_points,
                             itpGather, itpScatter, itpSymmetric)
-from .neighbor import (LBVH_find_nearest, LBVH_find_nearest_h, LBVH_query, LinearBVH, LinearBVH_build,
+from .neighbor import (LBVH_find_nearest, LBVH_find_nearest_h, LBVH_probe_neighbors, LBVH_query, LinearBVH,
+                       LinearBVH_build,
                        MortonEncoding, NeighborSelection, traversal_stats)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -17,6 +17,8 @@ PB_ERR_CAPACITY = -2
 PB_ERR_CUDA = -3
 PB_ERR_STATE = -4
 PB_ERR_INTERNAL = -6
+PB_ERR_KEY = -7
+PB_ERR_DIMENSION = -8
 PB_FP64 = 0
 PB_FP32C = 1
 PB_PERMUTE_CALLER = 1
@@ -58,10 +60,11 @@ class PBCatalog(ctypes.Structure):
 
 
 EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set_option", "pb_linear_bvh",
-            "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors", "pb_traversal_stats",
+            "pb_export_encoding", "pb_export_tree", "pb_find_nearest_h", "pb_query_count", "pb_query_neighbors",
+            "pb_probe_neighbors", "pb_traversal_stats",
             "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
             "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc",
-            "pb_last_schedule", "pb_scheduler_features", "pb_scheduler_set", "pb_scheduler_get",
+            "pb_last_schedule", "pb_last_pair_split", "pb_scheduler_features", "pb_scheduler_set", "pb_scheduler_get",
             "pb_scheduler_predict", "pb_scheduler_gradients", "pb_scheduler_train", "pb_grid_points"]
 
 SCHED_FEATURES = 16
@@ -92,6 +95,7 @@ def load():
         "pb_find_nearest_h": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
         "pb_query_count": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
         "pb_query_neighbors": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+        "pb_probe_neighbors": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
         "pb_traversal_stats": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int32, _vp]),
         "pb_interpolate_points": (ctypes.c_int32, [_vp, P(PBCatalog), ctypes.c_int64, _vp, _vp, _vp,
                                                    ctypes.c_int32, ctypes.c_int32, P(_vp)]),
@@ -105,6 +109,7 @@ def load():
         "pb_launch_count": (ctypes.c_int64, [_vp]),
         "pb_last_timings": (ctypes.c_int32, [_vp, _dp, _dp, _lp]),
         "pb_last_schedule": (ctypes.c_int32, [_vp, _lp, _lp, _lp, _dp]),
+        "pb_last_pair_split": (ctypes.c_int32, [_vp, _lp, _lp, _lp, _lp]),
         "pb_grid_points": (ctypes.c_int32, [_vp, ctypes.c_int32, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp,
                                             ctypes.c_int64, _vp, _vp, _vp]),
         "pb_scheduler_features": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp]),
@@ -173,9 +178,11 @@ class Handle:
         msg = "%s: %s" % (what, self.error())
         if rc == PB_ERR_CAPACITY:
             raise CapacityError(msg)
+        if rc == PB_ERR_KEY:
+            raise KeyError(msg)
+        if rc == PB_ERR_DIMENSION:
+            raise DimensionMismatch(msg)
         if rc == PB_ERR_INVALID:
-            if "KeyError" in msg:
-                raise KeyError(msg)
             raise ArgumentError(msg)
         if rc == PB_ERR_STATE:
             raise ArgumentError(msg)
@@ -200,6 +207,13 @@ class Handle:
         r, d, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         self.lib.pb_last_schedule(self.h, ctypes.byref(r), ctypes.byref(d), ctypes.byref(c), None)
         return r.value, d.value, c.value
+
+    def pair_split(self):
+        """(heavy queries, light queries, heavy pairs, light pairs) of the last point call: heavy
+        queries were summed by the FP32-compensated pair kernel, light ones by the FP64 one."""
+        v = [ctypes.c_int64() for _ in range(4)]
+        self.lib.pb_last_pair_split(self.h, *[ctypes.byref(x) for x in v])
+        return tuple(x.value for x in v)
 
     def phase_times(self):
         """Device ms of the nearest search, walk and pair sums, summed over slices and rounds (option "timing")."""

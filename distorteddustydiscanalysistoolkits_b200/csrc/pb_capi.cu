@@ -53,22 +53,31 @@ int fail(Handle &H, int code, const std::string &msg)
             return fail(H, PB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));         \
     } while (0)
 
-bool is_device_ptr(const void *p)
+// Where a caller pointer lives: 0 host memory (pageable or pinned), 1 device memory of the
+// handle's device or managed memory, 2 device memory of another GPU (rejected: the kernels
+// would read it without peer access).
+int ptr_place(const Handle &H, const void *p)
 {
-    if (!p) return false;
+    if (!p) return 0;
     cudaPointerAttributes a;
     cudaError_t e = cudaPointerGetAttributes(&a, p);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return 0;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return 1;
+    if (a.type == cudaMemoryTypeDevice) return a.device == H.device ? 1 : 2;
+    return 0;
 }
+
+bool is_device_ptr(const Handle &H, const void *p) { return ptr_place(H, p) == 1; }
 
 // device view of a caller array: the array itself if it lives on the device, else a staged copy
 cudaError_t stage_in(Handle &H, DBuf &buf, const void *p, size_t bytes, const void **out)
 {
-    if (is_device_ptr(p)) {
+    const int place = ptr_place(H, p);
+    if (place == 2) return cudaErrorInvalidDevice;
+    if (place == 1) {
         *out = p;
         return cudaSuccess;
     }
@@ -87,7 +96,8 @@ int check_status(Handle &H)
     if (st & ST_NONFINITE) return fail(H, PB_ERR_INVALID, "non-finite particle coordinate or smoothing length");
     if (st & ST_REFIT) return fail(H, PB_ERR_INTERNAL, "LBVH refit: an internal node was not combined exactly twice");
     if (st & ST_TRAVERSAL) return fail(H, PB_ERR_INTERNAL, "traversal exceeded its iteration bound");
-    if (st & ST_POOL) return fail(H, PB_ERR_INVALID, "neighbour pool offsets too small for a query");
+    if (st & ST_POOL)
+        return fail(H, PB_ERR_DIMENSION, "neighbour pool offsets too small for a query (DimensionMismatch)");
     return PB_OK;
 }
 
@@ -143,14 +153,14 @@ int validate_catalog(Handle &H, const pb_catalog *c, bool lines)
         return fail(H, PB_ERR_INVALID, "LineSamples interpolation takes scalar quantities only");
     auto okcol = [&](int col) { return col >= 0 && col < H.ncol; };
     for (int i = 0; i < c->n_scalar; ++i)
-        if (!okcol(c->scalar_cols[i])) return fail(H, PB_ERR_INVALID, "scalar column out of range (KeyError)");
+        if (!okcol(c->scalar_cols[i])) return fail(H, PB_ERR_KEY, "scalar column out of range (KeyError)");
     for (int i = 0; i < c->n_grad; ++i)
         if (c->grad_cols[i] != -1 && !okcol(c->grad_cols[i]))
-            return fail(H, PB_ERR_INVALID, "gradient column out of range (KeyError)");
+            return fail(H, PB_ERR_KEY, "gradient column out of range (KeyError)");
     for (int i = 0; i < 3 * c->n_div; ++i)
-        if (!okcol(c->div_cols[i])) return fail(H, PB_ERR_INVALID, "divergence column out of range (KeyError)");
+        if (!okcol(c->div_cols[i])) return fail(H, PB_ERR_KEY, "divergence column out of range (KeyError)");
     for (int i = 0; i < 3 * c->n_curl; ++i)
-        if (!okcol(c->curl_cols[i])) return fail(H, PB_ERR_INVALID, "curl column out of range (KeyError)");
+        if (!okcol(c->curl_cols[i])) return fail(H, PB_ERR_KEY, "curl column out of range (KeyError)");
     return PB_OK;
 }
 
@@ -311,7 +321,8 @@ int stage_outputs(Handle &H, int64_t L, int64_t npts, double *const *out, std::v
     if ((int64_t)H.q_outs.size() < L) H.q_outs.resize(L);
     for (int64_t l = 0; l < L; ++l) {
         if (!out || !out[l]) return fail(H, PB_ERR_INVALID, "output pointer is NULL");
-        if (is_device_ptr(out[l])) dev[l] = out[l];
+        if (ptr_place(H, out[l]) == 2) return fail(H, PB_ERR_INVALID, "output is device memory of another GPU");
+        if (is_device_ptr(H, out[l])) dev[l] = out[l];
         else {
             CK(H.q_outs[l].reserve(sizeof(double) * npts));
             dev[l] = H.q_outs[l].as<double>();
@@ -489,7 +500,7 @@ int reserve_pool(Handle &H, int64_t m, int ns)
         cap /= 2;
     }
     H.pool_cap = cap;
-    CK(H.pool_ctr.reserve(32));
+    CK(H.pool_ctr.reserve(64));   // [0] chunks used, [1] deferred | heavy count, [2] walk queue, [4..5] pair split
     CK(H.items.reserve(sizeof(int2) * m * ns));
     CK(H.wbnear.reserve(sizeof(int) * m));
     CK(H.qacc.reserve(sizeof(unsigned) * m));
@@ -521,7 +532,13 @@ int fused_fallback(Handle &H, const DevTree &T, const std::vector<Launch> &launc
     CK(cudaMemcpyAsync(list.data(), lst, sizeof(uint32_t) * nd, cudaMemcpyDeviceToHost, H.stream));
     CK(cudaMemcpyAsync(acc.data(), P.qacc, sizeof(unsigned) * nd, cudaMemcpyDeviceToHost, H.stream));
     CK(cudaStreamSynchronize(H.stream));
-    for (int64_t k = 0; k < nd; ++k) (acc[k] > (unsigned)H.light_max ? heavy : light).push_back(list[k]);
+    for (int64_t k = 0; k < nd; ++k) {
+        const bool hv = acc[k] > (unsigned)H.light_max;
+        (hv ? heavy : light).push_back(list[k]);
+        (hv ? H.split_hp : H.split_lp) += acc[k];
+    }
+    H.split_hq += (int64_t)heavy.size();
+    H.split_lq += (int64_t)light.size();
     uint32_t *hl = lst, *ll = lst + heavy.size();
     if (!heavy.empty())
         CK(cudaMemcpyAsync(hl, heavy.data(), sizeof(uint32_t) * heavy.size(), cudaMemcpyHostToDevice, H.stream));
@@ -628,6 +645,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
         s0 += m;
         for (int round = 0;; ++round) {
             CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
+            CK(cudaMemsetAsync(ctr + 4, 0, 16, H.stream));
             CK(cudaMemsetAsync(H.qacc.p, 0, sizeof(unsigned) * m, H.stream));
             CK(cudaMemsetAsync(H.qflag.p, 0, sizeof(int) * m, H.stream));
             RunPool P;
@@ -670,7 +688,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             H.interp_launches++;
             uint32_t *order = nullptr;
             int64_t m_heavy = 0;
-            CK(launch_split_order(&H, P, m, (unsigned)H.light_max, mode == 0, &order, &m_heavy));
+            CK(launch_split_order(&H, P, m, (unsigned)H.light_max, mode == 0, &order, &m_heavy, ctr + 4));
             ev_record(H, 6);
             if (m_heavy > 0)
                 for (const Launch &Lc : launches) {
@@ -685,10 +703,14 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                     H.interp_launches++;
                 }
             ev_record(H, 7);
-            unsigned long long used_nd[2] = {0, 0};
-            CK(cudaMemcpyAsync(used_nd, ctr, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, H.stream));
+            unsigned long long used_nd[6] = {0, 0, 0, 0, 0, 0};
+            CK(cudaMemcpyAsync(used_nd, ctr, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, H.stream));
             CK(cudaStreamSynchronize(H.stream));
             const unsigned nd = (unsigned)(used_nd[1] & 0xffffffffULL);
+            H.split_hq += m_heavy;
+            H.split_lq += m - (int64_t)nd - m_heavy;
+            H.split_hp += (int64_t)used_nd[4];
+            H.split_lp += (int64_t)used_nd[5];
             if (round == 0) {
                 // next slice: the queries that 85 % of the pool holds at this slice's chunks per query
                 const unsigned long long used = std::min<unsigned long long>(used_nd[0], H.pool_cap);
@@ -741,6 +763,7 @@ int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, 
     if (npts < 0) return fail(H, PB_ERR_INVALID, "negative number of sample points");
     H.interp_launches = 0;
     H.t_interp_ms = 0.f;
+    H.split_hq = H.split_lq = H.split_hp = H.split_lp = 0;
     int64_t L = catalog_L(cat);
     if (npts == 0 || L == 0) return PB_OK;
     if (!qx || !qy || !qz) return fail(H, PB_ERR_INVALID, "sample coordinate pointer is NULL");
@@ -751,12 +774,12 @@ int do_points(Handle &H, const pb_catalog *cat, int64_t npts, const double *qx, 
     std::vector<double *> dev;
     std::vector<int> is_host;
     if ((rc = stage_outputs(H, L, npts, out, dev, is_host))) return rc;
-    const uint32_t *perm;
-    if ((rc = query_order(H, npts, dx, dy, dz, &perm))) return rc;
     DevTree T = make_tree(H);
     std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
     std::vector<Launch> launches64 = plan(items_of(cat, false));
-    ev_record(H, 2);
+    ev_record(H, 2);   // the query ordering is part of the timed interpolation
+    const uint32_t *perm;
+    if ((rc = query_order(H, npts, dx, dy, dz, &perm))) return rc;
     if (precision == PB_FP64) {
         // every query summed by the FP64 pair kernel (the fused kernel's arithmetic, bit for bit)
         const int64_t keep = H.light_max;
@@ -801,7 +824,8 @@ int do_lines(Handle &H, const pb_catalog *cat, int64_t nl, const double *ox, con
     const double *dirs[3] = {mx, my, mz};
     const void *dv[3];
     for (int d = 0; d < 3; ++d) {
-        if (is_device_ptr(dirs[d])) dv[d] = dirs[d];
+        if (ptr_place(H, dirs[d]) == 2) return fail(H, PB_ERR_INVALID, "direction is device memory of another GPU");
+        if (is_device_ptr(H, dirs[d])) dv[d] = dirs[d];
         else {
             CK(cudaMemcpyAsync(stage + d * nl, dirs[d], sizeof(double) * nl, cudaMemcpyHostToDevice, H.stream));
             dv[d] = stage + d * nl;
@@ -811,11 +835,11 @@ int do_lines(Handle &H, const pb_catalog *cat, int64_t nl, const double *ox, con
     std::vector<double *> dev;
     std::vector<int> is_host;
     if ((rc = stage_outputs(H, L, nl, out, dev, is_host))) return rc;
-    const uint32_t *perm;
-    if ((rc = query_order(H, nl, dox, doy, doz, &perm))) return rc;
     DevTree T = make_tree(H);
     std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
-    ev_record(H, 2);
+    ev_record(H, 2);   // the line ordering is part of the timed interpolation
+    const uint32_t *perm;
+    if ((rc = query_order(H, nl, dox, doy, doz, &perm))) return rc;
     for (const Launch &Lc : launches) {
         DevCatalog C = dev_catalog(H, Lc, dev.data());
         if (precision == PB_FP64)
@@ -1001,7 +1025,7 @@ int32_t pb_query_count(pb_handle *h, int64_t npts, const double *qx, const doubl
     CK(stage_in(H, H.q_aux, radius, 8 * npts, &r));
     CK(H.q_out.reserve(8 * npts));
     CK(launch_query(&H, make_tree(H), npts, dx, dy, dz, (const double *)r, nullptr, H.q_out.as<int64_t>(), nullptr,
-                    nullptr));
+                    nullptr, nullptr));
     CK(cudaMemcpyAsync(counts, H.q_out.p, 8 * npts, cudaMemcpyDefault, H.stream));
     return check_status(H);
 }
@@ -1026,7 +1050,7 @@ int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const d
     CK(cudaStreamSynchronize(H.stream));
     CK(cudaMemcpy(&total, (const int64_t *)o + npts, 8, cudaMemcpyDefault));
     if (total < 0) return fail(H, PB_ERR_INVALID, "negative pool size");
-    bool pool_dev = is_device_ptr(pool);
+    bool pool_dev = is_device_ptr(H, pool);
     int64_t *dpool = pool;
     if (!pool_dev) {
         CK(H.q_perm_alt.reserve(8 * (total + 1)));
@@ -1034,9 +1058,34 @@ int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const d
     }
     CK(H.q_out.reserve(8 * npts));
     CK(launch_query(&H, make_tree(H), npts, dx, dy, dz, (const double *)r, (const int64_t *)o, nullptr, dpool,
-                    H.q_out.as<int64_t>()));
+                    H.q_out.as<int64_t>(), nullptr));
     if (!pool_dev && total > 0) CK(cudaMemcpyAsync(pool, dpool, 8 * total, cudaMemcpyDeviceToHost, H.stream));
     if (nearest) CK(cudaMemcpyAsync(nearest, H.q_out.p, 8 * npts, cudaMemcpyDefault, H.stream));
+    return check_status(H);
+}
+
+int32_t pb_probe_neighbors(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                           const double *radius, int64_t *count, int64_t *closest_idx, double *closest_d2)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!H.built) return fail(H, PB_ERR_STATE, "no LBVH has been built on this handle");
+    if (npts <= 0) return npts == 0 ? PB_OK : fail(H, PB_ERR_INVALID, "negative npts");
+    if (!radius) return fail(H, PB_ERR_INVALID, "NULL radius");
+    CK(cudaSetDevice(H.device));
+    CK(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream));
+    const double *dx, *dy, *dz;
+    int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
+    if (rc) return rc;
+    const void *r;
+    CK(stage_in(H, H.q_aux, radius, 8 * npts, &r));
+    CK(H.q_out.reserve(24 * npts));
+    int64_t *dc = H.q_out.as<int64_t>(), *di = dc + npts;
+    double *dd = reinterpret_cast<double *>(di + npts);
+    CK(launch_query(&H, make_tree(H), npts, dx, dy, dz, (const double *)r, nullptr, dc, nullptr, di, dd));
+    if (count) CK(cudaMemcpyAsync(count, dc, 8 * npts, cudaMemcpyDefault, H.stream));
+    if (closest_idx) CK(cudaMemcpyAsync(closest_idx, di, 8 * npts, cudaMemcpyDefault, H.stream));
+    if (closest_d2) CK(cudaMemcpyAsync(closest_d2, dd, 8 * npts, cudaMemcpyDefault, H.stream));
     return check_status(H);
 }
 
@@ -1055,7 +1104,7 @@ int32_t pb_traversal_stats(pb_handle *h, int64_t npts, const double *qx, const d
     int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
     if (rc) return rc;
     int64_t *ds = stats;
-    bool dev = is_device_ptr(stats);
+    bool dev = is_device_ptr(H, stats);
     if (!dev) {
         CK(H.q_aux.reserve(40 * npts));
         ds = H.q_aux.as<int64_t>();
@@ -1127,7 +1176,7 @@ int32_t pb_grid_points(pb_handle *h, int32_t coord, const double *a0, int64_t n0
     CK(cudaMemcpyAsync(ax + n0 + n1, a2, sizeof(double) * n2, cudaMemcpyDefault, H.stream));
     double *outs[3] = {x, y, z};
     double *dst[3];
-    const bool dev = is_device_ptr(x) && is_device_ptr(y) && is_device_ptr(z);
+    const bool dev = is_device_ptr(H, x) && is_device_ptr(H, y) && is_device_ptr(H, z);
     if (!dev) {
         CK(H.grid_out.reserve(sizeof(double) * 3 * n));
         for (int d = 0; d < 3; ++d) dst[d] = H.grid_out.as<double>() + d * n;
@@ -1147,7 +1196,7 @@ namespace {
 // device view of a float array given as host or device memory (staged into `buf`)
 int stage_f32(Handle &H, DBuf &buf, const float *src, int64_t n, const float **out)
 {
-    if (is_device_ptr(src)) {
+    if (is_device_ptr(H, src)) {
         *out = src;
         return PB_OK;
     }
@@ -1188,7 +1237,7 @@ int32_t pb_scheduler_features(pb_handle *h, int64_t npts, const double *qx, cons
     int rc = stage_queries(H, npts, qx, qy, qz, &dx, &dy, &dz);
     if (rc) return rc;
     float *out = feat;
-    if (!is_device_ptr(feat)) {
+    if (!is_device_ptr(H, feat)) {
         CK(H.sched_feat.reserve(sizeof(float) * SCHED_F * npts));
         out = H.sched_feat.as<float>();
     }
@@ -1305,6 +1354,17 @@ int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *defe
     if (walk_rounds) *walk_rounds = h->H.walk_rounds;
     if (deferred) *deferred = h->H.deferred_total;
     if (pool_chunks) *pool_chunks = (int64_t)h->H.pool_cap;
+    return PB_OK;
+}
+
+int32_t pb_last_pair_split(const pb_handle *h, int64_t *heavy_queries, int64_t *light_queries, int64_t *heavy_pairs,
+                           int64_t *light_pairs)
+{
+    if (!h) return PB_ERR_INVALID;
+    if (heavy_queries) *heavy_queries = h->H.split_hq;
+    if (light_queries) *light_queries = h->H.split_lq;
+    if (heavy_pairs) *heavy_pairs = h->H.split_hp;
+    if (light_pairs) *light_pairs = h->H.split_lp;
     return PB_OK;
 }
 

@@ -88,6 +88,9 @@ struct Handle {
     int sched_nclass = 16;
     unsigned long long pool_cap = 0;
     int64_t walk_rounds = 0, deferred_total = 0;
+    // queries and accepted pairs of the last point call summed by the FP32C (heavy) and the
+    // FP64 (light) pair kernels
+    int64_t split_hq = 0, split_lq = 0, split_hp = 0, split_lp = 0;
 
     // query-side scratch
     DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
@@ -132,7 +135,7 @@ cudaError_t launch_walk_list(Handle *H, const DevTree &T, int strategy, const Ru
                              unsigned long long *counter);
 cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **order);
 cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned light_max, bool plain,
-                               uint32_t **order, int64_t *m_heavy);
+                               uint32_t **order, int64_t *m_heavy, unsigned long long *pairs);
 cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out);
 
 // ---- launchers (pb_sched.cu) ----
@@ -171,7 +174,7 @@ cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double
                            const double *qz, double *h_out, int64_t *idx_out);
 cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
                          const double *qz, const double *radius, const int64_t *offsets, int64_t *counts,
-                         int64_t *pool, int64_t *nearest);
+                         int64_t *pool, int64_t *nearest, double *nearest_d2);
 cudaError_t launch_grid_points(Handle *H, int coord, const double *a0, int64_t n0, const double *a1, int64_t n1,
                                const double *a2, int64_t n2, double *x, double *y, double *z);
 cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, const double *qx, const double *qy,

@@ -20,7 +20,9 @@
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current); make that first
 //     call before any stream capture is started on the device.
-//   * Inputs and outputs are device pointers supplied by the caller.
+//   * Inputs and outputs are device pointers of the current device, supplied by the caller.
+//   * A CUDA error still pending from the caller's own earlier work makes the call return
+//     PB_ERR_CUDA before it launches anything; the error is left for the caller to read.
 #include <cstdint>
 #include <mutex>
 
@@ -55,12 +57,14 @@ struct QP {
     int flat[3];
 };
 
-// per-axis min/max in one block (order independent), then the quantisation parameters of
+// per-axis min/max in one block (order independent: exact comparisons), reduced with warp
+// shuffles and one value per warp in shared memory, then the quantisation parameters of
 // MortonCode.jl:443-456; non-finite coordinates set the status word
 __global__ void k_na_bbox(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
                           const double *__restrict__ z, QP *qp, int *status)
 {
-    __shared__ double smin[3][1024], smax[3][1024];
+    __shared__ double smin[3][32], smax[3][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     int bad = 0;
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
@@ -72,23 +76,33 @@ __global__ void k_na_bbox(int64_t n, const double *__restrict__ x, const double 
         }
     }
     if (bad) atomicOr(status, 1);
-    for (int d = 0; d < 3; ++d) { smin[d][threadIdx.x] = mn[d]; smax[d][threadIdx.x] = mx[d]; }
+    for (int off = 16; off > 0; off >>= 1)
+        for (int d = 0; d < 3; ++d) {
+            const double a = __shfl_xor_sync(0xffffffffu, mn[d], off), b = __shfl_xor_sync(0xffffffffu, mx[d], off);
+            if (a < mn[d]) mn[d] = a;
+            if (b > mx[d]) mx[d] = b;
+        }
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) { smin[d][warp] = mn[d]; smax[d][warp] = mx[d]; }
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if ((int)threadIdx.x < s)
-            for (int d = 0; d < 3; ++d) {
-                if (smin[d][threadIdx.x + s] < smin[d][threadIdx.x]) smin[d][threadIdx.x] = smin[d][threadIdx.x + s];
-                if (smax[d][threadIdx.x + s] > smax[d][threadIdx.x]) smax[d][threadIdx.x] = smax[d][threadIdx.x + s];
-            }
-        __syncthreads();
+    if (warp != 0) return;
+    for (int d = 0; d < 3; ++d) {
+        mn[d] = lane < nwarps ? smin[d][lane] : INFINITY;
+        mx[d] = lane < nwarps ? smax[d][lane] : -INFINITY;
     }
-    if (threadIdx.x < 3) {
-        int d = threadIdx.x;
-        double dv = smax[d][0] - smin[d][0];
-        qp->vmin[d] = smin[d][0];
-        qp->flat[d] = (dv == 0.0);
-        qp->inv[d] = (dv == 0.0) ? 0.0 : 1.0 / dv;
-    }
+    for (int off = 16; off > 0; off >>= 1)
+        for (int d = 0; d < 3; ++d) {
+            const double a = __shfl_xor_sync(0xffffffffu, mn[d], off), b = __shfl_xor_sync(0xffffffffu, mx[d], off);
+            if (a < mn[d]) mn[d] = a;
+            if (b > mx[d]) mx[d] = b;
+        }
+    if (lane == 0)
+        for (int d = 0; d < 3; ++d) {
+            const double dv = mx[d] - mn[d];
+            qp->vmin[d] = mn[d];
+            qp->flat[d] = (dv == 0.0);
+            qp->inv[d] = (dv == 0.0) ? 0.0 : 1.0 / dv;
+        }
 }
 
 __device__ __forceinline__ uint64_t na_expand(uint64_t v)
@@ -242,14 +256,17 @@ __global__ void k_na_dedupe(int64_t n, uint64_t *keys, const uint32_t *__restric
     }
 }
 
-bool is_device(const void *p)
+// The GPU a pointer's memory belongs to: its device id for device memory, -2 for managed
+// memory (usable from any device), -1 for host memory or an unknown pointer.
+int device_of(const void *p)
 {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return -1;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return -2;
+    return a.type == cudaMemoryTypeDevice ? a.device : -1;
 }
 
 std::mutex g_setup_mutex;
@@ -262,10 +279,18 @@ extern "C" int32_t pb_morton_sort_noalloc(const double *x, const double *y, cons
 {
     if (n < 1 || !x || !y || !z || !codes_out || !order_out) return PB_ERR_INVALID;
     if (n > NA_MAX_N) return PB_ERR_CAPACITY;
-    if (!is_device(x) || !is_device(y) || !is_device(z) || !is_device(codes_out) || !is_device(order_out))
-        return PB_ERR_INVALID;
+    const void *ptrs[5] = {x, y, z, codes_out, order_out};
+    int owner[5];
+    for (int k = 0; k < 5; ++k)
+        if ((owner[k] = device_of(ptrs[k])) == -1) return PB_ERR_INVALID;   // host memory
+    // an error still pending from the caller's earlier work is left in place for the caller
+    // and reported before any launch, so that it is not taken for one of this call's
+    if (cudaPeekAtLastError() != cudaSuccess) return PB_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PB_ERR_CUDA;
+    // memory of another GPU is refused: the kernels would read it without peer access
+    for (int k = 0; k < 5; ++k)
+        if (owner[k] >= 0 && owner[k] != dev) return PB_ERR_INVALID;
     unsigned char *base;
     {
         // once per device, with that device current: the device address of the static array

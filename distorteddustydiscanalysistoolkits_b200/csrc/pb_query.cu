@@ -19,10 +19,13 @@ __global__ void k_nearest(DevTree T, int64_t nq, const double *__restrict__ qx, 
     }
 }
 
-// gather predicate d2 <= radius^2 (LinearBVHTraversalMacros.jl:26-108); pool == nullptr counts only
+// gather predicate d2 <= radius^2 (LinearBVHTraversalMacros.jl:26-108); pool == nullptr counts only.
+// The closest accepted leaf is the first strictly closer one in DFS order (LinearBVHQueries.jl:33-39,
+// 196-203): nearest[i] its index (-1 if none), nearest_d2[i] its squared distance (+Inf if none).
 __global__ void k_query(DevTree T, int64_t nq, const double *__restrict__ qx, const double *__restrict__ qy,
                         const double *__restrict__ qz, const double *__restrict__ radius,
-                        const int64_t *__restrict__ offsets, int64_t *counts, int64_t *pool, int64_t *nearest)
+                        const int64_t *__restrict__ offsets, int64_t *counts, int64_t *pool, int64_t *nearest,
+                        double *nearest_d2)
 {
     const int64_t n = T.n;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x) {
@@ -58,6 +61,7 @@ __global__ void k_query(DevTree T, int64_t nq, const double *__restrict__ qx, co
         }
         if (counts) counts[i] = cnt;
         if (nearest) nearest[i] = ci;
+        if (nearest_d2) nearest_d2[i] = cd;
     }
 }
 
@@ -167,10 +171,10 @@ cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double
 
 cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
                          const double *qz, const double *radius, const int64_t *offsets, int64_t *counts,
-                         int64_t *pool, int64_t *nearest)
+                         int64_t *pool, int64_t *nearest, double *nearest_d2)
 {
     k_query<<<grid_for(nq, 128, 1 << 30), 128, 0, H->stream>>>(T, nq, qx, qy, qz, radius, offsets, counts, pool,
-                                                                nearest);
+                                                                nearest, nearest_d2);
     H->launches += 1;
     return cudaGetLastError();
 }

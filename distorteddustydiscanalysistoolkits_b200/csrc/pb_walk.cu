@@ -266,15 +266,46 @@ __global__ void k_lpt_keys(int64_t m, const unsigned *__restrict__ qacc, const i
     }
 }
 
-// queries (not deferred) with more than `light_max` accepted leaves; one atomic per block
+// queries (not deferred) with more than `light_max` accepted leaves, and the accepted pairs of
+// the heavy and of the light queries (pairs[0], pairs[1]); one set of atomics per block
 __global__ void k_count_heavy(int64_t m, const unsigned *__restrict__ qacc, const int *__restrict__ qflag,
-                              unsigned light_max, unsigned *count)
+                              unsigned light_max, unsigned *count, unsigned long long *pairs)
 {
-    for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < m; base += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t j = base + threadIdx.x;
-        const int heavy = j < m && !qflag[j] && qacc[j] > light_max;
-        const int c = __syncthreads_count(heavy);
-        if (threadIdx.x == 0 && c) atomicAdd(count, (unsigned)c);
+    __shared__ unsigned long long s_pairs[2];
+    __shared__ unsigned s_count;
+    if (threadIdx.x == 0) {
+        s_pairs[0] = s_pairs[1] = 0ULL;
+        s_count = 0u;
+    }
+    __syncthreads();
+    unsigned c = 0;
+    unsigned long long ph = 0, pl = 0;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+        if (qflag[j]) continue;
+        const unsigned a = qacc[j];
+        if (a > light_max) {
+            ++c;
+            ph += a;
+        } else {
+            pl += a;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        c += __shfl_down_sync(0xffffffffu, c, off);
+        ph += __shfl_down_sync(0xffffffffu, ph, off);
+        pl += __shfl_down_sync(0xffffffffu, pl, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (c) atomicAdd(&s_count, c);
+        if (ph) atomicAdd(&s_pairs[0], ph);
+        if (pl) atomicAdd(&s_pairs[1], pl);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_count) atomicAdd(count, s_count);
+        if (s_pairs[0]) atomicAdd(pairs, s_pairs[0]);
+        if (s_pairs[1]) atomicAdd(pairs + 1, s_pairs[1]);
     }
 }
 
@@ -429,9 +460,10 @@ cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **
 }
 
 // pair order of a walked slice and the number of heavy queries at its front: heaviest first
-// (LPT) unless `plain`, where it is the stable heavy/light partition of the walk order
+// (LPT) unless `plain`, where it is the stable heavy/light partition of the walk order; the
+// accepted pairs of the heavy and the light queries are added to pairs[0], pairs[1]
 cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned light_max, bool plain,
-                               uint32_t **order, int64_t *m_heavy)
+                               uint32_t **order, int64_t *m_heavy, unsigned long long *pairs)
 {
     cudaError_t e;
     if (!plain) {
@@ -452,7 +484,7 @@ cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned 
     }
     unsigned *cnt = reinterpret_cast<unsigned *>(P.n_deferred) + 1;
     if ((e = cudaMemsetAsync(cnt, 0, sizeof(unsigned), H->stream))) return e;
-    k_count_heavy<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, light_max, cnt);
+    k_count_heavy<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, light_max, cnt, pairs);
     H->launches += 1;
     if ((e = cudaGetLastError())) return e;
     unsigned hcount = 0;

@@ -6,6 +6,7 @@
   LBVH_find_nearest_h      LinearBVHQueries.jl:118-140 (batched)
   LBVH_find_nearest        LinearBVHQueries.jl:79-95 (batched; leaf index)
   LBVH_query               LBVH_query! LinearBVHQueries.jl:183-211 + NeighborSelection.jl:1-23 (batched)
+  LBVH_probe_neighbors     LinearBVHQueries.jl:22-42 (batched)
 
 Indices are 0-based (Julia's are 1-based); node ids keep the reference's unified
 1-based id space.
@@ -145,3 +146,19 @@ def LBVH_query(lbvh, points, radius):
     H.check(H.lib.pb_query_neighbors(H.h, n, ptr(qx), ptr(qy), ptr(qz), r.ctypes.data, offsets.ctypes.data,
                                      pool.ctypes.data, nearest.ctypes.data), "LBVH_query!")
     return [NeighborSelection(pool[offsets[i]:offsets[i + 1]], counts[i], nearest[i]) for i in range(n)]
+
+
+def LBVH_probe_neighbors(lbvh, points, radius):
+    """Batched LBVH_probe_neighbors: for every point the number of leaves within ``radius``
+    (d2 <= radius^2), the 0-based index of the closest of them (-1 if none; the reference's 0)
+    and its squared distance (+Inf if none; the reference's typemax).  Returns three arrays."""
+    qx, qy, qz = _pts(points)
+    n = len(qx)
+    r = np.broadcast_to(np.asarray(radius, np.float64), (n,)).copy()
+    count = np.empty(n, np.int64)
+    idx = np.empty(n, np.int64)
+    d2 = np.empty(n)
+    H = lbvh.handle
+    H.check(H.lib.pb_probe_neighbors(H.h, n, ptr(qx), ptr(qy), ptr(qz), r.ctypes.data, count.ctypes.data,
+                                     idx.ctypes.data, d2.ctypes.data), "LBVH_probe_neighbors")
+    return count, idx, d2

@@ -35,11 +35,15 @@ extern "C" {
 #endif
 
 #define PB_OK 0
-#define PB_ERR_INVALID (-1)   /* ArgumentError / DimensionMismatch / bad enum / non-finite coordinate */
+#define PB_ERR_INVALID (-1)   /* ArgumentError: bad value, bad enum, non-finite coordinate, n = 0 */
 #define PB_ERR_CAPACITY (-2)  /* n > 2^30 (BinaryRadixTree.jl:89-90) */
 #define PB_ERR_CUDA (-3)      /* CUDA runtime error (message in pb_last_error) */
 #define PB_ERR_STATE (-4)     /* query before pb_linear_bvh */
 #define PB_ERR_INTERNAL (-6)  /* device consistency check failed (refit counters, traversal bound) */
+#define PB_ERR_KEY (-7)       /* KeyError: a catalog column that the input does not have
+                                 (InterpolationCatalog.jl:161-176) */
+#define PB_ERR_DIMENSION (-8) /* DimensionMismatch: array lengths that do not agree (a neighbour
+                                 pool shorter than a query's count; InterpolationInput.jl:87-98) */
 
 #define PB_FP64 0
 #define PB_FP32C 1
@@ -113,6 +117,13 @@ int32_t pb_query_count(pb_handle *h, int64_t npts, const double *qx, const doubl
                        const double *radius, int64_t *counts);
 int32_t pb_query_neighbors(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
                            const double *radius, const int64_t *offsets, int64_t *pool, int64_t *nearest);
+/* LBVH_probe_neighbors (LinearBVHQueries.jl:22-42), batched: the gather traversal with
+   r2 = radius^2 counts the accepted leaves (count[i]) and keeps the first strictly closer one
+   in DFS order, i.e. the minimum squared distance and among equal distances the smallest
+   sorted index: closest_idx[i] (0-based; -1 if none, the reference's 0) and closest_d2[i]
+   (+Inf if none, the reference's typemax).  Any output may be NULL. */
+int32_t pb_probe_neighbors(pb_handle *h, int64_t npts, const double *qx, const double *qy, const double *qz,
+                           const double *radius, int64_t *count, int64_t *closest_idx, double *closest_d2);
 
 /* Event counts of the reference traversal algorithm on the last build (leaf size 1, Karras
    tree, left-first DFS, FP64 boxes; LinearBVHTraversalMacros.jl:26-371 driven as in
@@ -213,6 +224,12 @@ int32_t pb_scheduler_train(pb_handle *h, const float *X, const float *y, int64_t
    PB_RUN_POOL_MB (MiB) or PB_RUN_POOL_CHUNKS from the environment when set. */
 int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *deferred, int64_t *pool_chunks,
                          double *phase_ms);
+/* Diagnostics of the last point call (no counterpart in the reference): how the queries and
+   their accepted pairs were split between the FP32-compensated pair kernel (queries with more
+   than option "fp64_light_max" accepted neighbours; heavy) and the FP64 pair kernel (light).
+   In PB_FP64 mode every query is light.  Any output may be NULL. */
+int32_t pb_last_pair_split(const pb_handle *h, int64_t *heavy_queries, int64_t *light_queries, int64_t *heavy_pairs,
+                           int64_t *light_pairs);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,8 @@ def lib():
         L.orc_find_nearest_h.argtypes = [ctypes.POINTER(_Tree)] + [ctypes.c_double] * 3 + [_i64p]
         L.orc_query.restype = ctypes.c_int64
         L.orc_query.argtypes = [ctypes.POINTER(_Tree)] + [ctypes.c_double] * 4 + [_i64p, ctypes.c_int64, _i64p]
+        L.orc_probe_neighbors.restype = ctypes.c_int64
+        L.orc_probe_neighbors.argtypes = [ctypes.POINTER(_Tree)] + [ctypes.c_double] * 4 + [_i64p, _dp]
         L.orc_interp_points.restype = None
         L.orc_interp_points.argtypes = [ctypes.POINTER(_Tree), ctypes.POINTER(_Catalog), ctypes.c_int64,
                                         _dp, _dp, _dp, ctypes.c_int32, _dp, ctypes.c_int32, _i64p]
@@ -191,6 +193,15 @@ class OracleLBVH:
         cnt = lib().orc_query(ctypes.byref(t), float(p[0]), float(p[1]), float(p[2]), float(radius),
                               _p(pool, _i64p), self.n, ctypes.byref(nearest))
         return pool[:cnt].copy(), nearest.value
+
+    def probe_neighbors(self, p, radius):
+        """LBVH_probe_neighbors: (count, closest 0-based index or -1, closest d2 or +Inf)."""
+        t = self._geom_tree()
+        ci = ctypes.c_int64(-1)
+        cd = ctypes.c_double(0.0)
+        cnt = lib().orc_probe_neighbors(ctypes.byref(t), float(p[0]), float(p[1]), float(p[2]), float(radius),
+                                        ctypes.byref(ci), ctypes.byref(cd))
+        return cnt, ci.value, cd.value
 
     def interp_points(self, catalog, qx, qy, qz, strategy="itpSymmetric", nthreads=0, stats=False):
         qx, qy, qz = _f64(qx), _f64(qy), _f64(qz)

@@ -216,9 +216,13 @@ static inline uint64_t expand_bits3(uint64_t x)
     return x;
 }
 
+/* The per-particle loops of the build run on all host threads, as the reference's
+   Threads.@threads loops do (MortonCode.jl:301,484; BinaryRadixTree.jl:106-118); the
+   min/max reductions are exact, so the results do not depend on the thread count. */
 static void quantize_axis(int64_t n, const double *v, uint64_t *iv)
 {
     double vmin = v[0], vmax = v[0];
+#pragma omp parallel for reduction(min : vmin) reduction(max : vmax) schedule(static)
     for (int64_t i = 1; i < n; ++i) {
         if (v[i] < vmin) vmin = v[i];
         if (v[i] > vmax) vmax = v[i];
@@ -230,6 +234,7 @@ static void quantize_axis(int64_t n, const double *v, uint64_t *iv)
         return;
     }
     double inv = 1.0 / dv;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) {
         double f = (v[i] - vmin) * inv;
         iv[i] = (uint64_t)floor(scale * f);
@@ -328,6 +333,7 @@ int orc_build(int64_t n, const double *x, const double *y, const double *z, cons
     quantize_axis(n, x, ix);
     quantize_axis(n, y, iy);
     quantize_axis(n, z, iz);
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) {
         codes[i] = (expand_bits3(ix[i]) << 2) | (expand_bits3(iy[i]) << 1) | expand_bits3(iz[i]);
         order[i] = i;
@@ -337,6 +343,7 @@ int orc_build(int64_t n, const double *x, const double *y, const double *z, cons
     /* sequential duplicate bump (MortonCode.jl:189-193) */
     for (int64_t i = 1; i < n; ++i)
         if (codes[i] <= codes[i - 1]) codes[i] = codes[i - 1] + 1;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) {
         int64_t o = order[i];
         sx[i] = x[o]; sy[i] = y[o]; sz[i] = z[o]; sh[i] = h[o];
@@ -356,6 +363,7 @@ int orc_build(int64_t n, const double *x, const double *y, const double *z, cons
     int64_t nin = n - 1, off = n - 1;
     int32_t *range_hi = (int32_t *)malloc(sizeof(int32_t) * (size_t)(nin + 1));
     int32_t *adj = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+#pragma omp parallel for schedule(static)
     for (int64_t i = 1; i <= nin; ++i) {
         int64_t lo, hi;
         find_range(c1, n, i, &lo, &hi);
@@ -366,8 +374,10 @@ int orc_build(int64_t n, const double *x, const double *y, const double *z, cons
         int64_t ri = (s + 1 == hi) ? hi + off : s + 1;
         R[i] = (int32_t)ri; Pa[ri] = (int32_t)i;
     }
+#pragma omp parallel for schedule(static)
     for (int64_t i = 1; i <= n - 1; ++i) adj[i] = (int32_t)lcp(c1, i, i + 1);
     adj[n] = 2147483647;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 1; i <= nin; ++i) {
         int64_t hi = range_hi[i];
         if (hi == n) E[i] = 0;
@@ -377,6 +387,8 @@ int orc_build(int64_t n, const double *x, const double *y, const double *z, cons
             E[i] = (adj[nx] < adj[nx - 1]) ? (int32_t)(off + nx) : (int32_t)nx;
         }
     }
+    /* leaf escapes read only internal escapes, which are final here */
+#pragma omp parallel for schedule(static)
     for (int64_t id = n; id <= ntot; ++id) {
         int32_t p = Pa[id];
         if (p == 0) { E[id] = 0; continue; }
@@ -522,9 +534,11 @@ double orc_find_nearest_h(const orc_tree *t, double px, double py, double pz, in
     return nearest_h_impl(t, px, py, pz, best, NULL, NULL);
 }
 
-/* LBVH_query!: LinearBVHQueries.jl:183-205 */
-int64_t orc_query(const orc_tree *t, double px, double py, double pz, double radius,
-                  int64_t *pool, int64_t cap, int64_t *nearest)
+/* LBVH_query! (LinearBVHQueries.jl:183-205) and LBVH_probe_neighbors (LinearBVHQueries.jl:22-42):
+   the gather traversal with r2 = radius * radius; the closest accepted leaf is the first
+   strictly closer one in DFS order. */
+static int64_t query_impl(const orc_tree *t, double px, double py, double pz, double radius,
+                          int64_t *pool, int64_t cap, int64_t *nearest, double *nearest_d2)
 {
     double r2 = radius * radius, cd = INFINITY;
     int64_t count = 0, ci = -1, n = t->n;
@@ -556,7 +570,20 @@ int64_t orc_query(const orc_tree *t, double px, double py, double pz, double rad
         }
     }
     if (nearest) *nearest = ci;
+    if (nearest_d2) *nearest_d2 = cd;
     return count;
+}
+
+int64_t orc_query(const orc_tree *t, double px, double py, double pz, double radius,
+                  int64_t *pool, int64_t cap, int64_t *nearest)
+{
+    return query_impl(t, px, py, pz, radius, pool, cap, nearest, NULL);
+}
+
+int64_t orc_probe_neighbors(const orc_tree *t, double px, double py, double pz, double radius,
+                            int64_t *closest, double *closest_d2)
+{
+    return query_impl(t, px, py, pz, radius, NULL, 0, closest, closest_d2);
 }
 
 /* ------------------------------------------------------------------------------------ */

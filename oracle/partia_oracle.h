@@ -64,6 +64,11 @@ double orc_find_nearest_h(const orc_tree *t, double px, double py, double pz, in
 int64_t orc_query(const orc_tree *t, double px, double py, double pz, double radius,
                   int64_t *pool, int64_t cap, int64_t *nearest);
 
+/* LBVH_probe_neighbors: number of leaves within radius, the closest one (0-based, -1 if none)
+   and its squared distance (+Inf if none). */
+int64_t orc_probe_neighbors(const orc_tree *t, double px, double py, double pz, double radius,
+                            int64_t *closest, double *closest_d2);
+
 /* PointSamples interpolation on a built tree.  out is [L][npts].  stats (optional) is
    [npts][5]: nearest internal visits, nearest leaf tests, main internal visits,
    main leaf tests, accepted neighbours. */

@@ -2,7 +2,8 @@
 
 The reference is Julia and cannot run here, so no reference outputs exist; what its tests
 hold for this path are input fixtures and tabulated data.  This script reads them as text
-from the reference checkout (path given as argv[1], default /root/reference) and writes:
+from the reference checkout (its root given as argv[1] or by the PARTIA_REFERENCE environment
+variable) and writes:
 
   grid_interpolation_fixture.json  the 4-particle sets and sample templates of
       Partia.jl/test/grid_interpolation_test_common.jl:17-121
@@ -16,7 +17,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PARTIA_REFERENCE")
+if not REF:
+    sys.exit("usage: make_fixtures.py <reference checkout root>  (or set PARTIA_REFERENCE)")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -5,8 +5,9 @@ own all device memory through their own pool, or pipelines that cannot take an
 allocation's synchronisation).  Its scratch is a fixed static device array shared by all
 calls, so this test makes two calls in a row with different data and sizes and checks
 that each one reproduces, bit for bit, the Morton codes and sorting order that
-pb_linear_bvh + pb_export_encoding produce for the same particles, and that a size above
-the limit is refused.  It runs last (file name) so a failure here leaves every other GPU
+pb_linear_bvh + pb_export_encoding produce for the same particles -- at the largest size
+it accepts too -- that a size above the limit is refused, and that a non-finite
+coordinate is reported without spoiling the next call.  It runs last (file name) so a failure here leaves every other GPU
 test already run; it passes both alone and after the other tests.
 """
 import ctypes
@@ -67,3 +68,30 @@ def test_noalloc_rejects_oversize():
     out = torch.empty(n, dtype=torch.int64, device="cuda")
     rc = lib.pb_morton_sort_noalloc(t.data_ptr(), t.data_ptr(), t.data_ptr(), n, out.data_ptr(), out.data_ptr(), None)
     assert rc == _lib.PB_ERR_CAPACITY
+
+
+def test_noalloc_at_the_size_limit_then_nonfinite_then_again():
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    backend = pb.CUDAComputeBackend(0)
+    g = np.random.default_rng(7)
+    x, y, z = (np.ascontiguousarray(a) for a in g.uniform(-50, 50, (3, MAX_N)))
+    rc, codes, order = _noalloc(lib, x, y, z)
+    assert rc == _lib.PB_OK
+    exp_codes, exp_order = _regular(backend, x, y, z)
+    assert np.array_equal(codes, exp_codes) and np.array_equal(order, exp_order)
+    bad = x[:1000].copy()
+    bad[123] = np.nan
+    rc, _, _ = _noalloc(lib, bad, y[:1000], z[:1000])
+    assert rc == _lib.PB_ERR_INVALID
+    # the status word is cleared by the next call, which succeeds
+    rc, codes, order = _noalloc(lib, x[:1000], y[:1000], z[:1000])
+    assert rc == _lib.PB_OK
+    exp_codes, exp_order = _regular(backend, x[:1000], y[:1000], z[:1000])
+    assert np.array_equal(codes, exp_codes) and np.array_equal(order, exp_order)
+    # host memory is refused (the caller must pass device pointers)
+    out = np.empty(10, np.int64)
+    h = np.zeros(10)
+    assert lib.pb_morton_sort_noalloc(h.ctypes.data, h.ctypes.data, h.ctypes.data, 10, out.ctypes.data,
+                                      out.ctypes.data, None) == _lib.PB_ERR_INVALID
+    backend.close()
