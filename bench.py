@@ -24,8 +24,13 @@ kernel sums over the runs (FP32 compensated; FP64 for queries with <= 4096 neigh
             leaf test; main pass 36 B per internal visit + 28 B per leaf test + (2+k) x 4 B
             per accepted neighbour, k = quantity columns read) / traversal kernel time,
             against the measured HBM copy bandwidth
+  fp64      the same workload in FP64 mode (the reference's arithmetic) on the same GPU
+  c5        (one GPU, default run) the clumped 16M-particle disc: build ms, plain / tuned /
+            learned interpolation with identical-output hashes, pair roofline, FP32C error
+  cpu_baseline  the CPU oracle port on all host threads over a fixed seeded sample of 65,536
+            grid points (the sample's and the full grid's mean accepted neighbours beside it)
 --impl reference runs the CPU oracle port (the restated reference algorithm, all host
-threads) on a bounded sample of the same workload.
+threads) on the same fixed sample, dealt over the timed steps.
 """
 import argparse
 import datetime
@@ -63,7 +68,10 @@ def parse():
     ap.add_argument("--grid", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-mode timing of the same workload")
+    ap.add_argument("--no-c5", action="store_true", help="skip the clumped 16M-particle (C5) block of the default run")
+    ap.add_argument("--c5-grid", type=int, default=256, help="grid edge of the C5 block")
+    ap.add_argument("--c5-particles", type=int, default=1 << 24, help="particles of the C5 block")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-roofline", action="store_true", help="skip the event-count pass (profiling runs)")
     ap.add_argument("--json-out", default=None)
@@ -163,35 +171,34 @@ def algorithmic_bytes(stats, L, k_cols, s):
     return {"walk": nq * 24 + 32 * nv + 24 * nl + 36 * mv + 28 * ml, "pairs": nq * 8 * L + acc * (2 + k_cols) * s}
 
 
-def cpu_sample(n, m, seed):
-    """Seeded uniform sample of m grid points (sorted): the per-point work is heavy-tailed and
-    varies with position, so a random sample represents the grid better than a stride."""
+CPU_SAMPLE_POINTS = 65536
+CPU_SAMPLE_SEED = 2024
+
+
+def cpu_sample(n, m=CPU_SAMPLE_POINTS, seed=CPU_SAMPLE_SEED):
+    """The fixed seeded uniform sample of grid points the CPU oracle is timed on (sorted), the
+    same in the cpu_baseline leg and in the --impl reference arm: the per-point work is
+    heavy-tailed and varies with position, so a large random sample represents the grid."""
     g = np.random.default_rng(seed)
     return np.sort(g.choice(n, size=min(m, n), replace=False))
 
 
-def cpu_baseline(p, flat, cols, cat, seconds):
-    """Oracle port on the host cores: full build + a seeded random sample of the grid points."""
+def cpu_baseline(p, flat, cols, cat):
+    """Oracle port on all host cores: full LBVH build, then the fixed sample of grid points."""
     import oracle
     threads = oracle.max_threads()
     t0 = time.perf_counter()
     o = oracle.OracleLBVH(p["x"], p["y"], p["z"], p["h"]).attach(p["m"], p["rho"], [p[c] for c in cols])
     build_s = time.perf_counter() - t0
-    n = len(flat)
-    probe = cpu_sample(n, 2048, 12345)
+    idx = cpu_sample(len(flat))
     t0 = time.perf_counter()
-    o.interp_points(cat.oracle_dict(), *(c[probe] for c in flat.coor), strategy="itpSymmetric")
-    per = (time.perf_counter() - t0) / len(probe)
-    budget = max(seconds - build_s, 2.0)
-    m = int(min(n, max(2048, budget / max(per, 1e-9))))
-    idx = cpu_sample(n, m, 1)
-    t0 = time.perf_counter()
-    o.interp_points(cat.oracle_dict(), *(c[idx] for c in flat.coor), strategy="itpSymmetric")
+    _, st = o.interp_points(cat.oracle_dict(), *(c[idx] for c in flat.coor), strategy="itpSymmetric", stats=True)
     dt = time.perf_counter() - t0
     return {"value": len(idx) / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "oracle (C, OpenMP, FP64) on %d of %d grid points (seeded uniform sample), after a full "
-                      "%d-particle LBVH build (%.0f ms)" % (len(idx), n, len(p["x"]), build_s * 1e3),
-            "build_ms": build_s * 1e3}
+            "sample": "oracle (C, OpenMP, FP64) on a fixed seeded uniform sample of %d of %d grid points (seed %d), "
+                      "after a full %d-particle LBVH build (%.0f ms)" % (len(idx), len(flat), CPU_SAMPLE_SEED,
+                                                                         len(p["x"]), build_s * 1e3),
+            "build_ms": build_s * 1e3, "sample_mean_accepted": float(st[:, 4].mean())}
 
 
 def run_reference(args, rank, world):
@@ -204,29 +211,32 @@ def run_reference(args, rank, world):
     t0 = time.perf_counter()
     o = oracle.OracleLBVH(p["x"], p["y"], p["z"], p["h"]).attach(p["m"], p["rho"], [p[c] for c in cols])
     build_ms = (time.perf_counter() - t0) * 1e3
-    n = len(flat)
-    # bounded sample per step: about 3 s of CPU work, a different seeded uniform sample each step
-    probe = cpu_sample(n, 2048, 12345)
-    t0 = time.perf_counter()
-    o.interp_points(cat.oracle_dict(), *(c[probe] for c in flat.coor), strategy="itpSymmetric")
-    per = (time.perf_counter() - t0) / len(probe)
-    S = int(min(n, max(2048, 3.0 / max(per, 1e-9))))
-    times = []
-    for step in range(args.warmup + args.steps):
-        idx = cpu_sample(n, S, 100 + step)
+    idx = cpu_sample(len(flat))
+    # the fixed sample is dealt round-robin over the timed steps (each step a representative
+    # part of it), so all timed steps together evaluate exactly the cpu_baseline sample;
+    # warm-up steps take small slices of it
+    steps = max(1, args.steps)
+    for w in range(args.warmup):
+        o.interp_points(cat.oracle_dict(), *(c[idx[w::steps * 8][:256]] for c in flat.coor), strategy="itpSymmetric")
+    times, acc = [], []
+    for k in range(steps):
+        part = idx[k::steps]
         t0 = time.perf_counter()
-        o.interp_points(cat.oracle_dict(), *(c[idx] for c in flat.coor), strategy="itpSymmetric")
-        if step >= args.warmup:
-            times.append(time.perf_counter() - t0)
-    ms = 1e3 * float(np.mean(times))
-    value = S / (ms / 1e3)
-    sample = "%d of %d grid points per step (a seeded uniform sample, different each step); LBVH build of all " \
-             "%d particles once (%.0f ms)" % (S, n, len(p["x"]), build_ms)
+        _, st = o.interp_points(cat.oracle_dict(), *(c[part] for c in flat.coor), strategy="itpSymmetric", stats=True)
+        times.append(time.perf_counter() - t0)
+        acc.append(st[:, 4])
+    total = float(np.sum(times))
+    value = len(idx) / total
+    ms = 1e3 * total / steps
+    sample = ("fixed seeded uniform sample of %d of %d grid points (seed %d), dealt round-robin over the %d timed "
+              "steps; LBVH build of all %d particles once (%.0f ms)" % (len(idx), len(flat), CPU_SAMPLE_SEED, steps,
+                                                                         len(p["x"]), build_ms))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded disc)",
             "config": dict(config, precision="fp64"), "build_ms": build_ms,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "sample_mean_accepted": float(np.concatenate(acc).mean())},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference Julia code cannot run on this box (no Julia toolchain); this arm is the C "
                     "restatement of the reference algorithm (oracle/), OpenMP over all host threads"}
@@ -297,6 +307,110 @@ def run_lines(args, rank, world):
             with open(args.json_out, "w") as f:
                 f.write(json.dumps(line) + "\n")
     return 0
+
+
+def c5_block(local, model, sched_modes, args):
+    """The clumped-disc target measured inside the default run (one GPU): 2^24 particles (two
+    log spirals + 2000 clumps, C4 Wendland), rho + curl v on a 256^3 Cartesian grid, itpSymmetric,
+    FP32C.  Reports the LBVH build time (CUDA events, 10 builds), the interpolation time of the
+    plain, tuned and learned schedules (one timed run each after one warm-up run) with a hash
+    of each one's outputs (they must be identical), the pair kernels' roofline from the pair
+    phase time and the sample's accepted counts, and the FP32C error against the FP64 mode
+    (bit-exact with the oracle) on a seeded sample of 2^20 grid points."""
+    import ctypes
+    import hashlib
+    import torch
+    import distorteddustydiscanalysistoolkits_b200 as pb
+    from distorteddustydiscanalysistoolkits_b200 import _lib, accuracy, scheduler, synthetic
+    n = args.c5_particles
+    p = synthetic.clumped_disc(n, seed=5)
+    flat = pb.flatten(pb.Cartesian, synthetic.cartesian_box_grid(p, n=args.c5_grid))
+    npts = len(flat)
+    cols = synthetic.C2_COLUMNS
+    cat = pb.InterpolationCatalog(cols, scalars=("rho",), curls=("v",))
+    backend = pb.CUDAComputeBackend(local)
+    H = backend.handle
+    H.set_option("timing", 1)
+    if model is not None:
+        scheduler.set_model(H, model)
+    H.set_stream(torch.cuda.current_stream().cuda_stream)
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in p.items()}
+    q = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in flat.coor]
+    outs = [torch.empty(npts, dtype=torch.float64, device="cuda") for _ in range(cat.L)]
+    inp = pb.InterpolationInput(dev["x"], dev["y"], dev["z"], dev["m"], dev["h"], dev["rho"],
+                                tuple(dev[c] for c in cols), smoothed_kernel=pb.C4_Wendland)
+    cin, ccat = inp._c_struct(), cat._c_struct()
+    optrs = (ctypes.c_void_p * cat.L)(*[o.data_ptr() for o in outs])
+    qp = [c.data_ptr() for c in q]
+    builds = []
+    for k in range(12):
+        H.check(H.lib.pb_linear_bvh(H.h, ctypes.byref(cin), 0), "pb_linear_bvh")
+        if k >= 2:
+            builds.append(H.timings()[0])
+
+    def interp(prec=_lib.PB_FP32C):
+        H.check(H.lib.pb_interpolate_points(H.h, ctypes.byref(ccat), npts, qp[0], qp[1], qp[2], pb.itpSymmetric.code,
+                                            prec, optrs), "pb_interpolate_points")
+        return H.timings()[1]
+
+    runs = {}
+    H.set_option("schedule", scheduler.TUNED)
+    interp()   # warm-up: grows the run pool to its working size
+    for name in ("learned", "tuned", "plain"):
+        if name == "learned" and model is None:
+            continue
+        H.set_option("schedule", sched_modes[name])
+        ms = interp()
+        hs = hashlib.sha256()
+        for o in outs:
+            hs.update(o.cpu().numpy().tobytes())
+        ph = H.phase_times()
+        runs[name] = {"interp_ms": ms, "pts_per_s": npts / (ms / 1e3), "nearest_ms": ph[0], "walk_ms": ph[1],
+                      "pairs_ms": ph[2], "walk_rounds": H.schedule()[0], "deferred_queries": H.schedule()[1],
+                      "pair_split": dict(zip(("heavy_queries", "light_queries", "heavy_pairs", "light_pairs"),
+                                             H.pair_split())),
+                      "outputs_sha256": hs.hexdigest()}
+    H.set_option("schedule", scheduler.TUNED)
+    hashes = {r["outputs_sha256"] for r in runs.values()}
+    out = {"workload": "clumped disc, %d particles (2 log spirals + 2000 clumps, C4 Wendland), Cartesian %d^3 grid, "
+                       "itpSymmetric, rho + curl v (L=%d), FP32C" % (n, args.c5_grid, cat.L),
+           "build_ms": float(np.mean(builds)), "build_ms_min": float(np.min(builds)), "build_reps": len(builds),
+           "schedules": runs, "outputs_identical": len(hashes) == 1}
+    if "plain" in runs:
+        for name in runs:
+            out["%s_vs_plain" % name] = runs["plain"]["interp_ms"] / runs[name]["interp_ms"]
+    if "learned" in runs and "tuned" in runs:
+        out["learned_vs_tuned"] = runs["tuned"]["interp_ms"] / runs["learned"]["interp_ms"]
+    # accuracy and accepted counts on a seeded sample of grid points
+    g = np.random.default_rng(55)
+    idx = np.sort(g.choice(npts, size=min(npts, 1 << 20), replace=False))
+    qs = [torch.from_numpy(np.ascontiguousarray(c[idx])).cuda() for c in flat.coor]
+    lb = pb.LinearBVH(backend, n)
+    ref = pb.interpolate_points(lb, cat, qs, pb.itpSymmetric, pb.FP64)
+    got = pb.interpolate_points(lb, cat, qs, pb.itpSymmetric, pb.FP32C)
+    out["accuracy_fp32c_vs_fp64"] = accuracy.field_errors([a.cpu().numpy() for a in got],
+                                                          [r.cpu().numpy() for r in ref], cat.ordered_names)
+    out["accuracy_fp32c_vs_fp64"]["sample_points"] = len(idx)
+    st = pb.traversal_stats(lb, [c.cpu().numpy() for c in qs], pb.itpSymmetric)
+    mean_acc = float(st[:, 4].mean())
+    best = min(runs.values(), key=lambda r: r["interp_ms"]) if runs else None
+    if best is not None and best["pairs_ms"] > 0:
+        pair_bytes = npts * 8 * cat.L + mean_acc * npts * (2 + len(cols)) * 4
+        peak = _peak_gbs()
+        ach = pair_bytes / (best["pairs_ms"] / 1e3) / 1e9
+        out["roofline_pairs"] = {"achieved": ach, "peak": peak[0], "frac": ach / peak[0], "unit": "GB/s",
+                                 "peak_source": peak[1], "algorithmic_bytes": pair_bytes,
+                                 "mean_accepted_per_query_sample": mean_acc,
+                                 "note": "pair-phase bytes from the sample's mean accepted count x all grid points"}
+    backend.close()
+    return out
+
+
+def _peak_gbs():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    return 6650.0, "fallback 6.65 TB/s"
 
 
 def main():
@@ -419,9 +533,7 @@ def main():
         stats = pb.traversal_stats(lb, [c.cpu().numpy() for c in q], pb.itpSymmetric)
         s = 4 if prec == pb.FP32C else 8
         alg = algorithmic_bytes(stats, cat.L, len(cols), s)
-        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
-            os.path.join(REPO, "MEASURED_PEAKS.json")) else None
-        peak = peaks["hbm_gbs"] if peaks else 6650.0
+        peak, peak_source = _peak_gbs()
         ph = np.mean(np.array(main_phases), axis=0) if main_phases else np.zeros(3)
         kname = {"M4_spline": "M4", "C4_Wendland": "C4"}.get(config["kernel"], config["kernel"])
         pk = "k_pairs32w<itpSymmetric,%s> (+ k_pairs64w for light queries)" % kname if prec == pb.FP32C \
@@ -441,7 +553,7 @@ def main():
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None, "traffic": traffic,
                     "kernel": per[dom]["kernel"], "algorithmic_bytes_per_launch": alg[dom],
-                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6.65 TB/s",
+                    "peak_source": peak_source,
                     "phases": per,
                     "events_per_query": {k: float(stats[:, i].mean()) for i, k in enumerate(
                         ("nearest_internal", "nearest_leaf", "main_internal", "main_leaf", "accepted"))}}
@@ -490,9 +602,32 @@ def main():
                "path": "PointSamples_interpolation(CUDAComputeBackend) with pinned host arrays: H2D, build, "
                        "interpolation, D2H of outputs and of the permuted particle columns"}
 
+    # the same workload in FP64 mode (the reference's arithmetic, bit-exact with the oracle):
+    # the like-for-like GPU figure beside the FP64 CPU arm
+    fp64 = None
+    if prec == pb.FP32C and world == 1 and not args.no_fp64:
+        H.set_stream(stream.cuda_stream)
+        ts = []
+        for k in range(3):
+            flush.zero_()
+            rc = H.lib.pb_interpolate_points(H.h, ctypes.byref(ccat), npts, qp[0], qp[1], qp[2], pb.itpSymmetric.code,
+                                             _lib.PB_FP64, optrs)
+            H.check(rc, "pb_interpolate_points(FP64)")
+            if k > 0:
+                ts.append(H.timings()[1])
+        fp64 = {"interp_ms": float(np.mean(ts)), "pts_per_s": npts / (float(np.mean(ts)) / 1e3), "steps": len(ts),
+                "note": "FP64 mode on the same resident LBVH (every pair in the reference's FP64 arithmetic)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(p, flat, cols, cat, args.cpu_seconds)
+        cpu = cpu_baseline(p, flat, cols, cat)
+        if roofline is not None:
+            cpu["full_grid_mean_accepted"] = roofline["events_per_query"]["accepted"]
+
+    c5 = None
+    if rank == 0 and world == 1 and args.config == "c2" and not args.no_c5:
+        backend.close()
+        c5 = c5_block(local, model, sched_modes, args)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -503,7 +638,8 @@ def main():
                                l2_flush="256 MiB write between timed steps, outside the step events"),
                 "build_ms": build_ms, "interp_ms": interp_ms,
                 "pts_per_s_with_build": world * npts / (step_ms / 1e3),
-                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "fp64": fp64,
+                "c5": c5,
                 "schedule": dict(zip(("walk_rounds", "deferred_queries", "pool_chunks"), sched), mode=args.schedule),
                 "schedules": schedules,
                 "clocks": clocks, "accuracy_fp32c_vs_fp64": accuracy}
@@ -512,7 +648,8 @@ def main():
         if args.json_out:
             with open(args.json_out, "w") as f:
                 f.write(txt + "\n")
-    backend.close()
+    if c5 is None:
+        backend.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0

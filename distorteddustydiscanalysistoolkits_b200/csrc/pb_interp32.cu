@@ -92,11 +92,27 @@ __device__ __forceinline__ float ldexp_norm3(int k)
     }
 }
 
-// payload: record of `stride` float4s per sorted particle
+// payload: record of `stride` float4 fields per sorted particle
 //   [0] = {x_hi, y_hi, z_hi, 1/h}, [1] = {x_lo, y_lo, z_lo, m/rho}, [2] = {sigma h^-3, sigma h^-4, A0_hi, A0_lo},
 //   [3..] = remaining (hi, lo) column pairs.  Coordinates are double-float pairs, so the pair
 //   offset x_a - x_b is formed in FP32 as (xa_hi - xb_hi) + (xa_lo - xb_lo) without FP64 loads.
+// Layout: blocks of 32 consecutive particles, field-major inside a block -- field k of particle
+// b is float4 number ((b / 32) * stride + k) * 32 + b % 32.  The lanes of a warp read 32
+// consecutive particles (the common case: a batch inside one accepted run), so every field
+// load of the warp is one contiguous 512-byte segment.
 __host__ __device__ inline int payload_stride(int nU) { return 2 + (2 + 2 * nU + 3) / 4; }
+constexpr int PAY_BLOCK = 32;   // particles per payload block; field k is at rec[k * PAY_BLOCK]
+
+__host__ __device__ inline int64_t payload_float4s(int64_t n, int stride)
+{
+    return ((n + PAY_BLOCK - 1) / PAY_BLOCK) * PAY_BLOCK * stride;
+}
+
+// field 0 of particle b's record
+__device__ __forceinline__ const float4 *rec_of(const float4 *pay, int stride, int64_t b)
+{
+    return pay + (b >> 5) * (int64_t)(stride * PAY_BLOCK) + (b & (PAY_BLOCK - 1));
+}
 
 // Compile-time shape of a launch's catalog, for the pair kernels.  CAT 0 reads everything from
 // the DevCatalog at run time; 1: four columns, gradient + divergence + curl; 2: four columns,
@@ -144,10 +160,10 @@ __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int s
         double4 L = T.leaf[b];
         double ih = 1.0 / L.w;
         float xh = (float)L.x, yh = (float)L.y, zh = (float)L.z;
-        float4 *rec = pay + b * stride;
+        float4 *rec = const_cast<float4 *>(rec_of(pay, stride, b));
         rec[0] = make_float4(xh, yh, zh, (float)ih);
-        rec[1] = make_float4((float)(L.x - (double)xh), (float)(L.y - (double)yh), (float)(L.z - (double)zh),
-                             (float)(T.m[b] / T.rho[b]));
+        rec[PAY_BLOCK] = make_float4((float)(L.x - (double)xh), (float)(L.y - (double)yh), (float)(L.z - (double)zh),
+                                     (float)(T.m[b] / T.rho[b]));
         float v[2 + 2 * MAXU + 2];
         v[0] = (float)(sig * ih * ih * ih);
         v[1] = (float)(sig * ih * ih * ih * ih);
@@ -161,7 +177,7 @@ __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int s
         v[2 + 2 * MAXU] = 0.f;
         v[3 + 2 * MAXU] = 0.f;
         for (int k = 2; k < stride; ++k)
-            rec[k] = make_float4(v[4 * k - 8], v[4 * k - 7], v[4 * k - 6], v[4 * k - 5]);
+            rec[k * PAY_BLOCK] = make_float4(v[4 * k - 8], v[4 * k - 7], v[4 * k - 6], v[4 * k - 5]);
     }
 }
 
@@ -242,7 +258,7 @@ __device__ __forceinline__ void load_cols(const float4 *rec, int stride, float &
     float v[4 * 4];
 #pragma unroll
     for (int k = 2; k < 6; ++k) {
-        float4 c = (k < stride) ? __ldg(rec + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 c = (k < stride) ? __ldg(rec + k * PAY_BLOCK) : make_float4(0.f, 0.f, 0.f, 0.f);
         v[4 * k - 8] = c.x; v[4 * k - 7] = c.y; v[4 * k - 6] = c.z; v[4 * k - 5] = c.w;
     }
     cW = v[0];
@@ -262,8 +278,8 @@ __device__ __forceinline__ void terms32(const Acc32 &A, const DevCatalog &C, con
 {
     stride = CatShape<CAT>::stride(stride);
     const bool need_grad = CatShape<CAT>::any(C);
-    const float4 *rec = pay + b * stride;
-    const float4 p0 = __ldg(rec), p1 = __ldg(rec + 1);
+    const float4 *rec = rec_of(pay, stride, b);
+    const float4 p0 = __ldg(rec), p1 = __ldg(rec + PAY_BLOCK);
     const float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
     const float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
     const float dz = (Q.ph[2] - p0.z) + (Q.pl[2] - p1.z);
@@ -425,7 +441,7 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
         // quantities enter as offsets from the nearest particle's values, which are close
         // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
         float cw_, cg_;
-        load_cols<CAT>(pay + bnear * CatShape<CAT>::stride(stride), stride, cw_, cg_, A.hh, A.hl);
+        load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), bnear), stride, cw_, cg_, A.hh, A.hl);
         A.have = true;
     }
 }
@@ -434,7 +450,7 @@ template <int CAT>
 __device__ __forceinline__ void offsets_from(Acc32 &A, const float4 *pay, int stride, int64_t b0)
 {
     float cw_, cg_;
-    load_cols<CAT>(pay + b0 * CatShape<CAT>::stride(stride), stride, cw_, cg_, A.hh, A.hl);
+    load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), b0), stride, cw_, cg_, A.hh, A.hl);
     A.have = true;
 }
 
@@ -598,7 +614,7 @@ cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C,
                                int64_t npts)
 {
     int stride = payload_stride(C.nU);
-    cudaError_t e = H->payload.reserve(sizeof(float4) * stride * T.n);
+    cudaError_t e = H->payload.reserve(sizeof(float4) * payload_float4s(T.n, stride));
     if (e) return e;
     e = H->counter.reserve(sizeof(unsigned long long));
     if (e) return e;
@@ -658,7 +674,7 @@ cudaError_t launch_pairs_fp32(Handle *H, const DevTree &T, const DevCatalog &C, 
                               const double *qy, const double *qz)
 {
     int stride = payload_stride(C.nU);
-    cudaError_t e = H->payload.reserve(sizeof(float4) * stride * T.n);
+    cudaError_t e = H->payload.reserve(sizeof(float4) * payload_float4s(T.n, stride));
     if (e) return e;
     e = H->counter.reserve(sizeof(unsigned long long));
     if (e) return e;
