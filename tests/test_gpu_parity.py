@@ -5,10 +5,15 @@ neighbour lists (DFS order), and every FP64-mode interpolated value (the FP64 ke
 the reference's expressions in the reference's order, so equality is exact, NaN included).
 FP32-compensated mode: |gpu - oracle| <= 1e-5 * max|field| per field (the FP32 tolerance,
 scaled per field because several fields -- div v of a Keplerian flow, grad rho at the
-midplane -- pass through zero); for a field that does not change sign (the density) the
-pointwise relative error |gpu - oracle| / |oracle| <= 1e-5 at every point.  The pointwise
-relative error of every field is computed (accuracy.field_errors) and printed.  The FP32
-pair kernel itself is pinned by runs that send every query to it (option fp64_light_max = 0).
+midplane -- pass through zero).  With the default routing (queries of at most 4096 accepted
+neighbours summed in FP64) the density, a field that does not change sign, also meets
+|gpu - oracle| / |oracle| <= 1e-5 at every point.  The FP32 pair kernel itself is pinned by
+runs that send every query to it (option fp64_light_max = 0); there only the field-scaled
+bound is asserted: a query with a handful of neighbours near the edge of their support gets
+its value from kernel terms f(q) = (2 - q)^3 / 4 whose condition number 3q / (2 - q) grows
+without bound, so an FP32 evaluation of such a point can be off by far more than 1e-5 of its
+own (tiny) value -- the reason those queries are routed to FP64 by default.  The pointwise
+relative error of every field is computed (accuracy.field_errors) and printed.
 """
 import numpy as np
 import pytest
@@ -155,7 +160,7 @@ def _fp32c_run(backend, flat, inp, cat, strategy, light_max):
     return np.stack([g.grid for g in out.grids]), split
 
 
-def _check_fp32c(got, exp, names, positive=("rho",)):
+def _check_fp32c(got, exp, names, positive=()):
     assert np.array_equal(np.isnan(got), np.isnan(exp))
     st = accuracy.field_errors(got, exp, names)
     print({k: {m: "%.2e" % v[m] for m in ("max_field_scaled", "max_rel", "rms_rel") if m in v} for k, v in st.items()})
@@ -181,7 +186,7 @@ def test_points_fp32c_tolerance(backend, strategy, light_max):
     if light_max == 0:
         # the FP32 pair kernel summed every query that has a neighbour
         assert lp == 0 and hp > 0 and hq == int((st[:, 4] > 0).sum())
-    _check_fp32c(got, exp, cat.ordered_names)
+    _check_fp32c(got, exp, cat.ordered_names, positive=("rho",) if light_max else ())
 
 
 @pytest.mark.parametrize("light_max", [4096, 0])
@@ -194,7 +199,7 @@ def test_points_density_gradient_fp32c(backend, light_max):
     if light_max == 0:
         assert lp == 0 and hp > 0
     exp = _oracle(p).interp_points(cat.oracle_dict(), *flat.coor, strategy="itpSymmetric")
-    _check_fp32c(got, exp, cat.ordered_names)
+    _check_fp32c(got, exp, cat.ordered_names, positive=("rho",) if light_max else ())
 
 
 @pytest.mark.parametrize("kernel", ["M5_spline", "M6_spline", "C2_Wendland", "C4_Wendland", "C6_Wendland"])
