@@ -24,8 +24,8 @@ namespace pb {
 
 __device__ const float g_line_inorm32[6][PB_LINE_NTAB] = PB_LINE_INORM_INIT;
 
-constexpr int CHUNK = 8;
-static_assert(CHUNK % 2 == 0, "pairs of batches must not straddle a flush");
+constexpr int CHUNK = 16;
+static_assert(CHUNK % 4 == 0, "groups of two or four batches must not straddle a flush");
 
 // ---- kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) in FP32 ----
 // Algebraically identical to the reference's piecewise forms but arranged so that nothing
@@ -108,10 +108,10 @@ __host__ __device__ inline int64_t payload_float4s(int64_t n, int stride)
     return ((n + PAY_BLOCK - 1) / PAY_BLOCK) * PAY_BLOCK * stride;
 }
 
-// field 0 of particle b's record
-__device__ __forceinline__ const float4 *rec_of(const float4 *pay, int stride, int64_t b)
+// field 0 of particle b's record (b < n <= 2^30: 32-bit index arithmetic, one wide multiply)
+__device__ __forceinline__ const float4 *rec_of(const float4 *pay, int stride, uint32_t b)
 {
-    return pay + (b >> 5) * (int64_t)(stride * PAY_BLOCK) + (b & (PAY_BLOCK - 1));
+    return pay + (uint64_t)(b >> 5) * (uint32_t)(stride * PAY_BLOCK) + (b & (PAY_BLOCK - 1));
 }
 
 // Compile-time shape of a launch's catalog, for the pair kernels.  CAT 0 reads everything from
@@ -160,7 +160,7 @@ __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int s
         double4 L = T.leaf[b];
         double ih = 1.0 / L.w;
         float xh = (float)L.x, yh = (float)L.y, zh = (float)L.z;
-        float4 *rec = const_cast<float4 *>(rec_of(pay, stride, b));
+        float4 *rec = const_cast<float4 *>(rec_of(pay, stride, (uint32_t)b));
         rec[0] = make_float4(xh, yh, zh, (float)ih);
         rec[PAY_BLOCK] = make_float4((float)(L.x - (double)xh), (float)(L.y - (double)yh), (float)(L.z - (double)zh),
                                      (float)(T.m[b] / T.rho[b]));
@@ -274,7 +274,7 @@ struct Terms32 {
 
 template <int STRAT, int KT, int CAT>
 __device__ __forceinline__ void terms32(const Acc32 &A, const DevCatalog &C, const Query32 &Q,
-                                        const float4 *__restrict__ pay, int stride, int64_t b, Terms32 &t)
+                                        const float4 *__restrict__ pay, int stride, int b, Terms32 &t)
 {
     stride = CatShape<CAT>::stride(stride);
     const bool need_grad = CatShape<CAT>::any(C);
@@ -354,7 +354,7 @@ __device__ __forceinline__ void accum32(Acc32 &A, const DevCatalog &C, const Ter
 
 template <int STRAT, int KT, int CAT>
 __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, const Query32 &Q,
-                                       const float4 *__restrict__ pay, int stride, int64_t b)
+                                       const float4 *__restrict__ pay, int stride, int b)
 {
     Terms32 t;
     terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b, t);
@@ -365,7 +365,7 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, const Quer
 // in order -- the same arithmetic as two pair32 calls, with twice the independent work
 template <int STRAT, int KT, int CAT>
 __device__ __forceinline__ void pair32x2(Acc32 &A, const DevCatalog &C, const Query32 &Q,
-                                         const float4 *__restrict__ pay, int stride, int64_t b1, int64_t b2)
+                                         const float4 *__restrict__ pay, int stride, int b1, int b2)
 {
     Terms32 t1, t2;
     terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b1, t1);
@@ -441,13 +441,13 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
         // quantities enter as offsets from the nearest particle's values, which are close
         // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
         float cw_, cg_;
-        load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), bnear), stride, cw_, cg_, A.hh, A.hl);
+        load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), (uint32_t)bnear), stride, cw_, cg_, A.hh, A.hl);
         A.have = true;
     }
 }
 
 template <int CAT>
-__device__ __forceinline__ void offsets_from(Acc32 &A, const float4 *pay, int stride, int64_t b0)
+__device__ __forceinline__ void offsets_from(Acc32 &A, const float4 *pay, int stride, int b0)
 {
     float cw_, cg_;
     load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), b0), stride, cw_, cg_, A.hh, A.hl);
@@ -500,8 +500,8 @@ __global__ void __launch_bounds__(128) k_points32w(DevTree T, DevCatalog C, cons
         Slots S{0, -1};
         int nb = 0;   // full batches since the last flush (warp-uniform)
         auto proc = [&](int fill) {
-            if (!A.have) offsets_from<CAT_ANY>(A, pay, stride, __shfl_sync(0xffffffffu, S.mine, 0));
-            if (S.mine >= 0) pair32<STRAT, KT, CAT_ANY>(A, C, Q, pay, stride, S.mine);
+            if (!A.have) offsets_from<CAT_ANY>(A, pay, stride, (int)__shfl_sync(0xffffffffu, S.mine, 0));
+            if (S.mine >= 0) pair32<STRAT, KT, CAT_ANY>(A, C, Q, pay, stride, (int)S.mine);
             if (fill == 32 && ++nb == CHUNK) {
                 A.flush<CAT_ANY>(C);
                 nb = 0;
@@ -549,18 +549,18 @@ __global__ void __launch_bounds__(128, 5) k_pairs32w(DevTree T, DevCatalog C, co
         setup32<STRAT, CAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride,
                             s_acc + threadIdx.x);
         int nb = 0;   // full batches since the last flush (warp-uniform)
-        int64_t mine = -1;
-        auto first = [&](int64_t b0) {
+        int mine = -1;
+        auto first = [&](int b0) {
             if (!A.have) offsets_from<CAT>(A, pay, stride, b0);
         };
-        auto one = [&](int64_t b) {
+        auto one = [&](int b) {
             pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, b);
             if (++nb == CHUNK) {
                 A.flush<CAT>(C);
                 nb = 0;
             }
         };
-        auto two = [&](int64_t m1) {   // flush boundary after the second batch (nb is even here)
+        auto two = [&](int m1) {   // flush boundary after the second batch (nb is even here)
             pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
             nb += 2;
             if (nb == CHUNK) {
@@ -568,8 +568,18 @@ __global__ void __launch_bounds__(128, 5) k_pairs32w(DevTree T, DevCatalog C, co
                 nb = 0;
             }
         };
+        auto four = [&](int m1) {   // flush boundary after the fourth batch (nb is a multiple of 4 here)
+            pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
+            pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1 + 64, m1 + 96);
+            nb += 4;
+            if (nb == CHUNK) {
+                A.flush<CAT>(C);
+                nb = 0;
+            }
+        };
         auto cantwo = [&]() { return (nb & 1) == 0; };
-        deal_runs(P, j, lane, first, one, two, cantwo, mine);
+        auto canfour = [&]() { return (nb & 3) == 0; };
+        deal_runs(P, j, lane, first, one, two, cantwo, four, canfour, mine);
         if (mine >= 0) pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, mine);
         reduce_finalize32<CAT>(A, C, qi, lane);
     }

@@ -193,8 +193,11 @@ __global__ void __launch_bounds__(128) k_pairs64w(DevTree T, DevCatalog C, RunPo
             proc(32, m1 + 32);
         };
         auto cantwo = [&]() { return false; };
-        int64_t mine = -1;
-        const int fill = deal_runs(P, j, lane, first, one, two, cantwo, mine);
+        auto four = [&](int64_t m1) {
+            for (int k = 0; k < 4; ++k) proc(32, m1 + 32 * k);
+        };
+        int mine = -1;
+        const int fill = deal_runs(P, j, lane, first, one, two, cantwo, four, cantwo, mine);
         if (fill > 0) proc(fill, mine);
         double v[NT];
 #pragma unroll

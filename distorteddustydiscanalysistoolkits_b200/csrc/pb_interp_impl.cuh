@@ -380,13 +380,15 @@ __device__ __forceinline__ int64_t next_query(unsigned long long *counter, int l
 // k mod 32.  first(b) is called with the first leaf of every non-empty item (the callee uses
 // the very first one); one(mine) for every full batch (every lane holds a leaf); two(m1) for
 // two consecutive full batches inside one run (lane leaves m1 and m1 + 32) when cantwo()
-// allows it.  Within a chunk, lane l finds the run holding its leaf through a uniform run
-// cursor, or a binary search over the inclusive prefix sums of the run lengths held one per
-// lane when a batch spans several runs.  Returns the fill of the last, partial batch, whose
-// leaves are left in `mine` (-1 on empty lanes).
-template <typename FIRST, typename ONE, typename TWO, typename CANTWO>
+// allows it, and four(m1) for four of them (m1, m1 + 32, m1 + 64, m1 + 96) when canfour()
+// does.  Within a chunk, lane l finds the run holding its leaf through a uniform run cursor,
+// or a binary search over the inclusive prefix sums of the run lengths held one per lane
+// when a batch spans several runs.  Leaf indices are 32-bit (n <= 2^30), and so is every
+// count: an item's accepted leaves lie in one subtree.  Returns the fill of the last,
+// partial batch, whose leaves are left in `mine` (-1 on empty lanes).
+template <typename FIRST, typename ONE, typename TWO, typename CANTWO, typename FOUR, typename CANFOUR>
 __device__ __forceinline__ int deal_runs(const RunPool &P, int64_t j, int lane, FIRST &first, ONE &one, TWO &two,
-                                         CANTWO &cantwo, int64_t &mine)
+                                         CANTWO &cantwo, FOUR &four, CANFOUR &canfour, int &mine)
 {
     const int ns = P.ns;
     int fill = 0;
@@ -399,70 +401,76 @@ __device__ __forceinline__ int deal_runs(const RunPool &P, int64_t j, int lane, 
             nonempty &= nonempty - 1;
             int c = __shfl_sync(0xffffffffu, itm.x, l);
             int left = __shfl_sync(0xffffffffu, itm.y, l);
-            first(__ldg(&P.runs[(int64_t)c * RUN_CHUNK].x));
+            first((int)__ldg(&P.runs[(int64_t)c * RUN_CHUNK].x));
             while (left > 0) {
                 const int cnt = left < RUN_CHUNK ? left : RUN_CHUNK;
                 const uint2 rn = lane < cnt ? __ldg(P.runs + (int64_t)c * RUN_CHUNK + lane) : make_uint2(0u, 0u);
                 const int nextc = left > RUN_CHUNK ? __ldg(P.next + c) : -1;
-                unsigned inc = rn.y;
+                int inc = (int)rn.y;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
-                    unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+                    int v = __shfl_up_sync(0xffffffffu, inc, o);
                     if (lane >= o) inc += v;
                 }
-                const int64_t tot = __shfl_sync(0xffffffffu, inc, 31);
-                const unsigned ex_own = inc - rn.y;
-                int64_t tb = -fill;
+                const int tot = __shfl_sync(0xffffffffu, inc, 31);
+                const int ex_own = inc - (int)rn.y;
+                int tb = -fill;
                 // uniform cursor: run r0 holds leaf position max(tb, 0) of the chunk; a batch
                 // inside one run needs no search
                 int r0 = -1, rc = -1;
-                unsigned end0 = 0, lo0 = 0, ex0 = 0;
+                int end0 = 0, lo0 = 0, ex0 = 0;
                 for (;;) {
                     // t0 < tot = inc[cnt - 1], so the cursor stops at a run of this chunk
-                    const unsigned t0 = tb <= 0 ? 0u : (tb < tot ? (unsigned)tb : (unsigned)(tot - 1));
+                    const int t0 = tb <= 0 ? 0 : (tb < tot ? tb : tot - 1);
                     while (end0 <= t0 && r0 < 31) {
                         ++r0;
                         end0 = __shfl_sync(0xffffffffu, inc, r0);
                     }
-                    if (cantwo() && tb >= 0 && tb + 64 <= (int64_t)end0) {
-                        // two full batches inside one run
+                    if (tb >= 0 && tb + 64 <= end0) {
                         if (rc != r0) {
-                            lo0 = __shfl_sync(0xffffffffu, rn.x, r0);
+                            lo0 = __shfl_sync(0xffffffffu, (int)rn.x, r0);
                             ex0 = __shfl_sync(0xffffffffu, ex_own, r0);
                             rc = r0;
                         }
-                        const int64_t m1 = (int64_t)lo0 + ((unsigned)tb - ex0) + lane;
-                        two(m1);
-                        tb += 64;
-                        continue;   // the next pass assigns or closes what is left of the chunk
+                        const int m1 = lo0 + (tb - ex0) + lane;
+                        if (tb + 128 <= end0 && canfour()) {   // four full batches inside one run
+                            four(m1);
+                            tb += 128;
+                            continue;
+                        }
+                        if (cantwo()) {   // two full batches inside one run
+                            two(m1);
+                            tb += 64;
+                            continue;   // the next pass assigns or closes what is left of the chunk
+                        }
                     }
-                    if (tb >= 0 && tb + 32 <= (int64_t)end0) {
+                    if (tb >= 0 && tb + 32 <= end0) {
                         if (rc != r0) {
-                            lo0 = __shfl_sync(0xffffffffu, rn.x, r0);
+                            lo0 = __shfl_sync(0xffffffffu, (int)rn.x, r0);
                             ex0 = __shfl_sync(0xffffffffu, ex_own, r0);
                             rc = r0;
                         }
-                        mine = (int64_t)lo0 + ((unsigned)tb - ex0) + lane;
+                        mine = lo0 + (tb - ex0) + lane;
                     } else {
-                        const int64_t tl = tb + lane;
+                        const int tl = tb + lane;
                         const bool here = tl >= 0 && tl < tot;
-                        const unsigned tt = here ? (unsigned)tl : 0u;
+                        const int tt = here ? tl : 0;
                         int r = 0;
 #pragma unroll
                         for (int sh = 16; sh > 0; sh >>= 1) {
-                            unsigned v = __shfl_sync(0xffffffffu, inc, r + sh - 1);
+                            int v = __shfl_sync(0xffffffffu, inc, r + sh - 1);
                             if (v <= tt) r += sh;
                         }
-                        const unsigned lo = __shfl_sync(0xffffffffu, rn.x, r);
-                        const unsigned ex = __shfl_sync(0xffffffffu, ex_own, r);
-                        if (here) mine = (int64_t)lo + (tt - ex);
+                        const int lo = __shfl_sync(0xffffffffu, (int)rn.x, r);
+                        const int ex = __shfl_sync(0xffffffffu, ex_own, r);
+                        if (here) mine = lo + (tt - ex);
                     }
                     if (tb + 31 < tot) {
                         one(mine);   // full batch
                         mine = -1;
                         tb += 32;
                     } else {
-                        fill = (int)(tot - tb);
+                        fill = tot - tb;
                         break;
                     }
                 }
