@@ -255,16 +255,19 @@ def run_lines(args, rank, world):
     ng, nd = (args.particles or 6291456), (args.particles or 6291456) // 3
     npix = int(args.grid or 2048)
     gas, dust = synthetic.dusty_disc(ng, nd, seed=3 + rank, tilt_deg=30.0)
-    lines = synthetic.face_on_lines(gas, npix=npix)
-    nl = len(lines)
     prec = _lib.PB_FP32C if args.precision == "fp32c" else _lib.PB_FP64
     be = pb.CUDAComputeBackend(int(os.environ.get("LOCAL_RANK", "0")))
     H = be.handle
+    # the face-on image's lines are generated on the device (pb_line_image): origins on z = 0
+    # over the gas disc's x/y extent, direction (0, 0, 1)
+    xs = pb.grids.linrange(float(np.min(gas["x"])), float(np.max(gas["x"])), npix)
+    ys = pb.grids.linrange(float(np.min(gas["y"])), float(np.max(gas["y"])), npix)
+    lines = pb.LineSamples_image(be, xs, ys)
+    nl = len(lines)
     H.set_option("timing", 1)
     H.set_stream(torch.cuda.current_stream().cuda_stream)
     cat = pb.InterpolationCatalog(("rho", "vz"), scalars=("rho", "vz"))
-    o = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in lines.origin]
-    d = [torch.from_numpy(np.ascontiguousarray(c)).cuda() for c in lines.direction]
+    o, d = lines.origin, lines.direction
     species = []
     for sp in (gas, dust):
         dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in sp.items()}

@@ -10,7 +10,7 @@ from .grids import (Cartesian, Cylindrical, GridBundle, LineSamples, PointSample
                     StructuredGrid, coordinate_grid, flatten, restore_struct)
 from .interpolation import (C2_Wendland, C4_Wendland, C6_Wendland, CUDAComputeBackend, FP32C, FP64,
                             Greeting_CUDA, InterpolationCatalog, InterpolationInput, KernelFunctionValid, M4_spline,
-                            M5_spline, M6_spline, LineSamples_interpolation, PointSamples_interpolation,
+                            M5_spline, M6_spline, LineSamples_image, LineSamples_interpolation, PointSamples_interpolation,
                             StructuredGrid_interpolation, build_input, interpolate_lines, interpolate_points,
                             itpGather, itpScatter, itpSymmetric)
 from .neighbor import (LBVH_find_nearest, LBVH_find_nearest_h, LBVH_probe_neighbors, LBVH_query, LinearBVH,

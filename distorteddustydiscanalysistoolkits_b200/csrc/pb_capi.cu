@@ -5,6 +5,7 @@
 // launch's register budget is split into several traversal launches), device status
 // checks, and optional CUDA-event timing of the build and traversal stages.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -1187,6 +1188,51 @@ int32_t pb_grid_points(pb_handle *h, int32_t coord, const double *a0, int64_t n0
     if (!dev)
         for (int d = 0; d < 3; ++d)
             CK(cudaMemcpyAsync(outs[d], dst[d], sizeof(double) * n, cudaMemcpyDeviceToHost, H.stream));
+    CK(cudaStreamSynchronize(H.stream));
+    return PB_OK;
+}
+
+int32_t pb_line_image(pb_handle *h, const double *a0, int64_t n0, const double *a1, int64_t n1, const double *frame,
+                      double *ox, double *oy, double *oz, double *dx, double *dy, double *dz)
+{
+    if (!h) return PB_ERR_INVALID;
+    Handle &H = h->H;
+    if (!a0 || !a1 || !frame || !ox || !oy || !oz || !dx || !dy || !dz || n0 < 1 || n1 < 1)
+        return fail(H, PB_ERR_INVALID, "line image axes / outputs: bad arguments");
+    LineFrame F;
+    for (int d = 0; d < 3; ++d) {
+        F.c[d] = frame[d];
+        F.e1[d] = frame[3 + d];
+        F.e2[d] = frame[6 + d];
+        F.d[d] = frame[9 + d];
+    }
+    for (int k = 0; k < 12; ++k)
+        if (!std::isfinite(frame[k])) return fail(H, PB_ERR_INVALID, "line image frame is not finite");
+    const double dn = std::sqrt(F.d[0] * F.d[0] + F.d[1] * F.d[1] + F.d[2] * F.d[2]);
+    if (std::fabs(dn - 1.0) > 1e-12) return fail(H, PB_ERR_INVALID, "line direction must be a unit vector");
+    const int64_t n = n0 * n1;
+    CK(cudaSetDevice(H.device));
+    CK(H.grid_ax.reserve(sizeof(double) * (n0 + n1)));
+    double *ax = H.grid_ax.as<double>();
+    CK(cudaMemcpyAsync(ax, a0, sizeof(double) * n0, cudaMemcpyDefault, H.stream));
+    CK(cudaMemcpyAsync(ax + n0, a1, sizeof(double) * n1, cudaMemcpyDefault, H.stream));
+    double *outs[6] = {ox, oy, oz, dx, dy, dz};
+    double *dst[6];
+    bool dev = true;
+    for (int k = 0; k < 6; ++k) {
+        if (ptr_place(H, outs[k]) == 2) return fail(H, PB_ERR_INVALID, "output is device memory of another GPU");
+        dev = dev && is_device_ptr(H, outs[k]);
+    }
+    if (!dev) {
+        CK(H.grid_out.reserve(sizeof(double) * 6 * n));
+        for (int k = 0; k < 6; ++k) dst[k] = H.grid_out.as<double>() + k * n;
+    } else {
+        for (int k = 0; k < 6; ++k) dst[k] = outs[k];
+    }
+    CK(launch_line_image(&H, ax, n0, ax + n0, n1, F, dst[0], dst[1], dst[2], dst[3], dst[4], dst[5]));
+    if (!dev)
+        for (int k = 0; k < 6; ++k)
+            CK(cudaMemcpyAsync(outs[k], dst[k], sizeof(double) * n, cudaMemcpyDeviceToHost, H.stream));
     CK(cudaStreamSynchronize(H.stream));
     return PB_OK;
 }

@@ -179,6 +179,12 @@ cudaError_t launch_grid_points(Handle *H, int coord, const double *a0, int64_t n
                                const double *a2, int64_t n2, double *x, double *y, double *z);
 cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, const double *qx, const double *qy,
                          const double *qz, int64_t *stats);
+// image plane of pb_line_image: origin c, axes e1 and e2, line direction d
+struct LineFrame {
+    double c[3], e1[3], e2[3], d[3];
+};
+cudaError_t launch_line_image(Handle *H, const double *a0, int64_t n0, const double *a1, int64_t n1, const LineFrame &F,
+                              double *ox, double *oy, double *oz, double *dx, double *dy, double *dz);
 
 inline int grid_for(int64_t n, int block, int cap = 148 * 32)
 {

@@ -839,6 +839,19 @@ __device__ __forceinline__ R line_lut(const R *__restrict__ I, R qmax, R q)
     return __ldg(I + i - 1) * (R(1) - t) + __ldg(I + i) * t;
 }
 
+// FP32 table, index and interpolation fraction formed in FP64 from an FP64 q: near the support
+// edge the line-integrated kernel is small and steep, and an FP32 q / dq would move the
+// fraction by ~4e-4 of a table step
+__device__ __forceinline__ float line_lut_q64(const float *__restrict__ I, double qmax, double q)
+{
+    const double dq = qmax / double(PB_LINE_NTAB_DEV - 1);
+    const double idxf = q / dq + 1.0;
+    int i = (int)idxf;
+    i = i < 1 ? 1 : (i > PB_LINE_NTAB_DEV - 1 ? PB_LINE_NTAB_DEV - 1 : i);
+    const float t = (float)(idxf - (double)i);
+    return __ldg(I + i - 1) * (1.f - t) + __ldg(I + i) * t;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(128) k_lines(DevTree T, DevCatalog C, int64_t nl, const double *__restrict__ ox,
                                                const double *__restrict__ oy, const double *__restrict__ oz,
@@ -892,10 +905,11 @@ __global__ void __launch_bounds__(128) k_lines(DevTree T, DevCatalog C, int64_t 
                         for (int s = 0; s < MAXS; ++s)
                             if (s < C.n_scalar) acc[s] += __ldg(C.ucol[C.s_u[s]] + b) * w;
                     } else {
-                        float dr = sqrtf(d2 > 0.0 ? (float)d2 : 0.f);
-                        float invh = 1.f / (float)L.w;
-                        float q = dr * invh;
-                        float Iq = (q >= (float)K) ? 0.f : (float)line_lut<R>(I, qmax, (R)q);
+                        // the line distance and q in FP64 (the pair-distance part), the kernel
+                        // value and the sums in FP32
+                        const double q = sqrt(d2 > 0.0 ? d2 : 0.0) * (1.0 / L.w);
+                        const float invh = (float)(1.0 / L.w);
+                        float Iq = (q >= K) ? 0.f : line_lut_q64(reinterpret_cast<const float *>(I), K, q);
                         float w = (float)mb * (invh * Iq) / (float)rb;
                         cS1.add(w);
 #pragma unroll

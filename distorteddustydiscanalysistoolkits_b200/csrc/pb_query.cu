@@ -215,4 +215,30 @@ cudaError_t launch_grid_points(Handle *H, int coord, const double *a0, int64_t n
     return cudaGetLastError();
 }
 
+// Lines of an image (LineSamples of a column-density map): line k = i + n0 * j starts at
+// (c + a0[i] e1) + a1[j] e2 and runs along d; no FMA, so the values equal the host's
+// per-component expression.
+__global__ void k_line_image(const double *__restrict__ a0, int64_t n0, const double *__restrict__ a1, int64_t n1,
+                             LineFrame F, double *ox, double *oy, double *oz, double *dx, double *dy, double *dz)
+{
+    const int64_t n = n0 * n1;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const double u = a0[k % n0], v = a1[k / n0];
+        ox[k] = __dadd_rn(__dadd_rn(F.c[0], __dmul_rn(u, F.e1[0])), __dmul_rn(v, F.e2[0]));
+        oy[k] = __dadd_rn(__dadd_rn(F.c[1], __dmul_rn(u, F.e1[1])), __dmul_rn(v, F.e2[1]));
+        oz[k] = __dadd_rn(__dadd_rn(F.c[2], __dmul_rn(u, F.e1[2])), __dmul_rn(v, F.e2[2]));
+        dx[k] = F.d[0];
+        dy[k] = F.d[1];
+        dz[k] = F.d[2];
+    }
+}
+
+cudaError_t launch_line_image(Handle *H, const double *a0, int64_t n0, const double *a1, int64_t n1, const LineFrame &F,
+                              double *ox, double *oy, double *oz, double *dx, double *dy, double *dz)
+{
+    k_line_image<<<grid_for(n0 * n1, 256), 256, 0, H->stream>>>(a0, n0, a1, n1, F, ox, oy, oz, dx, dy, dz);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
 }  // namespace pb

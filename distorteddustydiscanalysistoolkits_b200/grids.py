@@ -30,6 +30,11 @@ class Spherical:      # (r, phi, theta)
 
 
 def _f64(a):
+    """float64, contiguous; a torch tensor (e.g. sample coordinates on the device) stays a tensor."""
+    if hasattr(a, "data_ptr") and hasattr(a, "is_contiguous"):
+        if str(a.dtype) != "torch.float64":
+            a = a.double()
+        return a.contiguous()
     return np.ascontiguousarray(a, dtype=np.float64)
 
 

@@ -328,14 +328,39 @@ def LineSamples_interpolation(backend, grid_template, input, catalog, itp_strate
         raise TypeError("LineSamples_interpolation takes a scalar-only catalog (MethodError in the reference)")
     H = backend.handle
     n = len(grid_template)
-    outs = _out_arrays(n, catalog.L)
-    cin, ccat = input._c_struct(), catalog._c_struct()
     o, d = grid_template.origin, grid_template.direction
+    outs = _out_arrays(n, catalog.L, like=o[0])
+    cin, ccat = input._c_struct(), catalog._c_struct()
     rc = H.lib.pb_line_samples_interpolation(H.h, ctypes.byref(cin), ctypes.byref(ccat), n, ptr(o[0]), ptr(o[1]),
                                              ptr(o[2]), ptr(d[0]), ptr(d[1]), ptr(d[2]), itpScatter.code,
                                              _precision(precision), _ptr_array(outs), _lib.PB_PERMUTE_CALLER)
     H.check(rc, "LineSamples_interpolation")
     return GridBundle([LineSamples(v, o, d) for v in outs], catalog.ordered_names)
+
+
+def LineSamples_image(backend, a0, a1, center=(0.0, 0.0, 0.0), e1=(1.0, 0.0, 0.0), e2=(0.0, 1.0, 0.0),
+                      direction=(0.0, 0.0, 1.0), on_device=True):
+    """The lines of an image, generated on the backend's device (pb_line_image): line
+    i + len(a0) * j starts at (center + a0[i] e1) + a1[j] e2 and runs along the unit vector
+    ``direction`` -- the LineSamples(xo, yo, zo, xd, yd, zd) a caller would build for a
+    column-density map (LineSamples.jl:391-403), without a host-to-device copy of 48 B per line
+    when ``on_device`` (origins and directions are then CUDA float64 tensors)."""
+    a0 = np.ascontiguousarray(a0, np.float64)
+    a1 = np.ascontiguousarray(a1, np.float64)
+    n = len(a0) * len(a1)
+    frame = np.ascontiguousarray(np.concatenate([center, e1, e2, direction]), np.float64)
+    if frame.shape != (12,):
+        raise ArgumentError("center, e1, e2 and direction must each have 3 components")
+    if on_device:
+        import torch
+        out = [torch.empty(n, dtype=torch.float64, device="cuda:%d" % backend.device) for _ in range(6)]
+    else:
+        out = [np.empty(n) for _ in range(6)]
+    H = backend.handle
+    H.check(H.lib.pb_line_image(H.h, ptr(a0), len(a0), ptr(a1), len(a1), ptr(frame), *[ptr(x) for x in out]),
+            "LineSamples_image")
+    vals = out[0].new_zeros(n) if on_device else np.zeros(n)
+    return LineSamples(vals, tuple(out[:3]), tuple(out[3:]))
 
 
 _COORD_CODE = {"Cartesian": 0, "Cylindrical": 2, "Spherical": 3}

@@ -192,6 +192,18 @@ int32_t pb_last_timings(const pb_handle *h, double *build_ms, double *interp_ms,
 int32_t pb_grid_points(pb_handle *h, int32_t coord, const double *a0, int64_t n0, const double *a1, int64_t n1,
                        const double *a2, int64_t n2, double *x, double *y, double *z);
 
+/* Lines of an image generated on the device: the LineSamples(xo, yo, zo, xd, yd, zd) a caller
+   builds for a column-density image (Partia.jl/src/julia/Grids/grids/LineSamples.jl:391-403;
+   the CUDA extension copies those host arrays to the device,
+   Partia.jl/ext/CUDAExt/Grids/grids/LineSamples.jl:1-7).  Line k = i + n0 * j (the first
+   axis fastest, as flatten orders a grid) starts at (c + a0[i] e1) + a1[j] e2 and runs along d,
+   evaluated per component without FMA.  frame holds 12 doubles (host memory): c, e1, e2, d;
+   d must be a unit vector (|d| within 1e-12 of 1; else PB_ERR_INVALID).  The face-on image of a
+   disc is c = (0, 0, z0), e1 = (1, 0, 0), e2 = (0, 1, 0), d = (0, 0, 1).  Axes may be host or
+   device arrays; with device outputs the lines never cross PCIe. */
+int32_t pb_line_image(pb_handle *h, const double *a0, int64_t n0, const double *a1, int64_t n1, const double *frame,
+                      double *ox, double *oy, double *oz, double *dx, double *dy, double *dz);
+
 /* Learned work prediction for the FP32-compensated point schedule (no counterpart in the
    reference; the reference runs queries in input order).  A 3-layer MLP of width 64 with
    BF16 weights and activations (PB_SCHED_FEATURES inputs, PB_SCHED_PARAMS parameters laid out

@@ -787,7 +787,9 @@ void orc_interp_points(const orc_tree *t, const orc_catalog *cat, int64_t npts,
     int64_t L = catalog_L(cat);
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+    /* one point per dispatch: the per-point work is heavy-tailed and neighbouring points are
+       alike, so larger chunks leave one thread finishing a run of heavy points alone */
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
 #endif
     for (int64_t i = 0; i < npts; ++i) {
         double o[4 * MAXQ + 4 * MAXQ];
@@ -856,7 +858,7 @@ void orc_interp_lines(const orc_tree *t, const orc_catalog *cat, int64_t nlines,
 {
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
 #endif
     for (int64_t i = 0; i < nlines; ++i) {
         double o[3] = {ox[i], oy[i], oz[i]}, m[3] = {dx[i], dy[i], dz[i]}, v[MAXQ];
