@@ -17,4 +17,7 @@ from .neighbor import (LBVH_find_nearest, LBVH_find_nearest_h, LBVH_probe_neighb
                        LinearBVH_build,
                        MortonEncoding, NeighborSelection, traversal_stats)
 
+from . import phantom
+from .phantom import MassFromColumn, MassFromParams, ParticleDataFrame, add_rho, read_phantom
+
 __all__ = [n for n in dir() if not n.startswith("_")]

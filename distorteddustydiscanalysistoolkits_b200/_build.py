@@ -31,6 +31,7 @@ UNITS = {
     "pb_interp32.cu": ["-fmad=false"],   # FMAs only where written (fmaf): bits independent of code shape
     "pb_capi.cu": [],
     "pb_noalloc.cu": ["-fmad=false"],
+    "pb_input.cu": ["-fmad=false"],
 }
 HEADERS = ["pb_device.cuh", "pb_internal.h", "pb_interp_impl.cuh", "line_tables.h"]
 

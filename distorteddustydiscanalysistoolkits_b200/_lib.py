@@ -65,7 +65,8 @@ EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set
             "pb_interpolate_points", "pb_interpolate_lines", "pb_point_samples_interpolation",
             "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc",
             "pb_last_schedule", "pb_last_pair_split", "pb_scheduler_features", "pb_scheduler_set", "pb_scheduler_get",
-            "pb_scheduler_predict", "pb_scheduler_gradients", "pb_scheduler_train", "pb_grid_points", "pb_line_image"]
+            "pb_scheduler_predict", "pb_scheduler_gradients", "pb_scheduler_train", "pb_grid_points", "pb_line_image",
+            "pb_column_to_f64", "pb_fill_f64", "pb_density_from_h"]
 
 SCHED_FEATURES = 16
 SCHED_PARAMS = 5313
@@ -113,6 +114,9 @@ def load():
         "pb_grid_points": (ctypes.c_int32, [_vp, ctypes.c_int32, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp,
                                             ctypes.c_int64, _vp, _vp, _vp]),
         "pb_line_image": (ctypes.c_int32, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp] + [_vp] * 6),
+        "pb_column_to_f64": (ctypes.c_int32, [_vp, _vp, ctypes.c_int32, ctypes.c_int64, _vp]),
+        "pb_fill_f64": (ctypes.c_int32, [_vp, ctypes.c_double, ctypes.c_int64, _vp]),
+        "pb_density_from_h": (ctypes.c_int32, [_vp, _vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double, _vp]),
         "pb_scheduler_features": (ctypes.c_int32, [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp]),
         "pb_scheduler_set": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_float, ctypes.c_int32]),
         "pb_scheduler_get": (ctypes.c_int32, [_vp, _vp]),

@@ -17,9 +17,6 @@
 
 using namespace pb;
 
-struct pb_handle {
-    Handle H;
-};
 
 pb::Handle::~Handle()
 {

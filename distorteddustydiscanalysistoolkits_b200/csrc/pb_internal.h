@@ -195,3 +195,8 @@ inline int grid_for(int64_t n, int block, int cap = 148 * 32)
 }
 
 }  // namespace pb
+
+// the opaque handle of the C ABI (include/partia_b200.h)
+struct pb_handle {
+    pb::Handle H;
+};

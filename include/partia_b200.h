@@ -204,6 +204,18 @@ int32_t pb_grid_points(pb_handle *h, int32_t coord, const double *a0, int64_t n0
 int32_t pb_line_image(pb_handle *h, const double *a0, int64_t n0, const double *a1, int64_t n1, const double *frame,
                       double *ox, double *oy, double *oz, double *dx, double *dy, double *dz);
 
+/* build_input on the device (ParticleIO.jl/src/julia/PartiaAdapter/build_input.jl:44-160):
+   the interpolation input's FP64 columns made from a snapshot's columns where they will be
+   used, so they cross PCIe in the width the dump stores them in (Phantom writes h and most
+   per-particle quantities as real*4).  All arrays are device memory of the handle's device.
+   pb_column_to_f64: dst[i] = src[i] widened to double (src_type 0 = float64, 1 = float32).
+   pb_fill_f64: dst[i] = value (a mass given once for all particles, MassFromParams).
+   pb_density_from_h: rho[i] = (mass hfact^3) (1/h[i])^3, add_rho! in 3D
+   (ParticleIO.jl/src/julia/Particles/add_quantities.jl:308-345), in its operation order. */
+int32_t pb_column_to_f64(pb_handle *h, const void *src, int32_t src_type, int64_t n, double *dst);
+int32_t pb_fill_f64(pb_handle *h, double value, int64_t n, double *dst);
+int32_t pb_density_from_h(pb_handle *h, const double *hsml, int64_t n, double mass, double hfact, double *rho);
+
 /* Learned work prediction for the FP32-compensated point schedule (no counterpart in the
    reference; the reference runs queries in input order).  A 3-layer MLP of width 64 with
    BF16 weights and activations (PB_SCHED_FEATURES inputs, PB_SCHED_PARAMS parameters laid out
