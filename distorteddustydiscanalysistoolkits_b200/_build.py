@@ -32,8 +32,10 @@ UNITS = {
     "pb_capi.cu": [],
     "pb_noalloc.cu": ["-fmad=false"],
     "pb_input.cu": ["-fmad=false"],
+    "pb_batch.cu": ["-fmad=false"],
 }
-HEADERS = ["pb_device.cuh", "pb_internal.h", "pb_interp_impl.cuh", "line_tables.h"]
+HEADERS = ["pb_device.cuh", "pb_internal.h", "pb_interp_impl.cuh", "pb_fp32_impl.cuh", "pb_fp64_impl.cuh",
+           "line_tables.h"]
 
 
 def _newer(target, deps):

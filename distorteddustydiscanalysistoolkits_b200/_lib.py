@@ -22,6 +22,8 @@ PB_ERR_DIMENSION = -8
 PB_FP64 = 0
 PB_FP32C = 1
 PB_PERMUTE_CALLER = 1
+PB_BUILD_ASYNC = 2
+PB_BATCH_ASYNC = 1
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -66,7 +68,7 @@ EXPORTED = ["pb_create", "pb_destroy", "pb_last_error", "pb_set_stream", "pb_set
             "pb_line_samples_interpolation", "pb_launch_count", "pb_last_timings", "pb_morton_sort_noalloc",
             "pb_last_schedule", "pb_last_pair_split", "pb_scheduler_features", "pb_scheduler_set", "pb_scheduler_get",
             "pb_scheduler_predict", "pb_scheduler_gradients", "pb_scheduler_train", "pb_grid_points", "pb_line_image",
-            "pb_column_to_f64", "pb_fill_f64", "pb_density_from_h"]
+            "pb_column_to_f64", "pb_fill_f64", "pb_density_from_h", "pb_batch_points", "pb_batch_check"]
 
 SCHED_FEATURES = 16
 SCHED_PARAMS = 5313
@@ -114,6 +116,9 @@ def load():
         "pb_grid_points": (ctypes.c_int32, [_vp, ctypes.c_int32, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp,
                                             ctypes.c_int64, _vp, _vp, _vp]),
         "pb_line_image": (ctypes.c_int32, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp] + [_vp] * 6),
+        "pb_batch_points": (ctypes.c_int32, [P(_vp), ctypes.c_int32, P(PBCatalog), _vp, _vp, _vp, _vp, _vp,
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+        "pb_batch_check": (ctypes.c_int32, [P(_vp), ctypes.c_int32]),
         "pb_column_to_f64": (ctypes.c_int32, [_vp, _vp, ctypes.c_int32, ctypes.c_int64, _vp]),
         "pb_fill_f64": (ctypes.c_int32, [_vp, ctypes.c_double, ctypes.c_int64, _vp]),
         "pb_density_from_h": (ctypes.c_int32, [_vp, _vp, ctypes.c_int64, ctypes.c_double, ctypes.c_double, _vp]),

@@ -10,17 +10,26 @@ separate calls (tests/test_gpu_batch.py).
 The autotuner times the interpolation of a representative job of each size class (particles
 and points rounded to powers of 4) under every candidate setting of the walk split, the slice
 size and the scheduler bin width, and keeps the fastest.
+
+``DeviceBatch`` is the one-launch form: every disc's particles, sample points and outputs stay
+on the device, each disc has its own handle (its tree), all handles share one stream, and a
+step enqueues every disc's LBVH build (PB_BUILD_ASYNC) and one pb_batch_points launch that
+interpolates the sample points of all discs.  The step can be captured in a CUDA graph and
+replayed.  ``BatchAutotuner`` picks its schedule options -- the walk's leaf size (subtrees of at
+most that many leaves scanned linearly), the disc order (given or most work first) and the
+blocks per SM -- by timing graph replays; outputs do not depend on them.
 """
+import ctypes
 import itertools
 import math
 import time
 
 import numpy as np
 
-from . import scheduler, synthetic
+from . import _lib, scheduler, synthetic
 from .grids import Cartesian, flatten
-from .interpolation import (C4_Wendland, InterpolationCatalog, InterpolationInput, M4_spline,
-                            PointSamples_interpolation, FP32C, itpSymmetric)
+from .interpolation import (C4_Wendland, CUDAComputeBackend, FP32C, FP64, InterpolationCatalog, InterpolationInput,
+                            M4_spline, PointSamples_interpolation, _precision, itpSymmetric)
 
 
 def c4_discs(n_discs=64, seed=100, n_min=50_000, n_max=4_000_000, edges=(32, 64, 128, 256)):
@@ -118,3 +127,132 @@ def batch_point_interpolation(backend, jobs, tuner=None, strategy=itpSymmetric, 
         b, i, _ = H.timings()
         ms.append({"build_ms": b, "interp_ms": i, "wall_ms": (time.perf_counter() - t0) * 1e3})
     return out, ms
+
+
+class DeviceBatch:
+    """Every job resident on one device, interpolated by one batched launch per step."""
+
+    def __init__(self, jobs, device=0, precision=FP32C, strategy=itpSymmetric):
+        import torch
+        if not jobs:
+            raise ValueError("no jobs")
+        self.torch = torch
+        self.device = device
+        self.precision = _precision(precision)
+        self.strategy = strategy
+        cat = jobs[0]["catalog"]
+        self.catalog = cat
+        self.L = cat.L
+        dev = "cuda:%d" % device
+        self.stream = torch.cuda.Stream(device=dev)
+        self.backends = [CUDAComputeBackend(device) for _ in jobs]
+        for b in self.backends:
+            b.handle.set_stream(self.stream.cuda_stream)
+        self.inputs, self.queries, self.outs, self.cin = [], [], [], []
+        for job in jobs:
+            inp = job["input"]
+            t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64)).to(dev)   # noqa: E731
+            d = InterpolationInput(t(inp.coord[0]), t(inp.coord[1]), t(inp.coord[2]), t(inp.m), t(inp.h), t(inp.rho),
+                                   tuple(t(q) for q in inp.quant), smoothed_kernel=inp.smoothed_kernel)
+            self.inputs.append(d)
+            self.cin.append(d._c_struct())
+            q = [t(c) for c in job["points"].coor]
+            self.queries.append(q)
+            self.outs.append([torch.empty(len(q[0]), dtype=torch.float64, device=dev) for _ in range(self.L)])
+        K = len(jobs)
+        self.K = K
+        self.ccat = cat._c_struct()
+        self.handles = (ctypes.c_void_p * K)(*[b.handle.h.value for b in self.backends])
+        self.npts = (ctypes.c_int64 * K)(*[len(q[0]) for q in self.queries])
+        self.qptr = [(ctypes.c_void_p * K)(*[q[d].data_ptr() for q in self.queries]) for d in range(3)]
+        self.optr = (ctypes.c_void_p * (K * self.L))(*[o.data_ptr() for outs in self.outs for o in outs])
+        self.lib = self.backends[0].handle.lib
+        self.graph = None
+
+    @property
+    def npoints(self):
+        return int(sum(self.npts))
+
+    def set_options(self, leaf_size=1, order=0, blocks_per_sm=0):
+        H = self.backends[0].handle
+        H.set_option("leaf_size", int(leaf_size))
+        H.set_option("batch_order", int(order))
+        H.set_option("batch_blocks_per_sm", int(blocks_per_sm))
+
+    def _enqueue(self, flags):
+        for b, cin in zip(self.backends, self.cin):
+            b.handle.check(self.lib.pb_linear_bvh(b.handle.h, ctypes.byref(cin), _lib.PB_BUILD_ASYNC), "LinearBVH!")
+        rc = self.lib.pb_batch_points(self.handles, self.K, ctypes.byref(self.ccat), self.npts, self.qptr[0],
+                                      self.qptr[1], self.qptr[2], self.optr, self.strategy.code, self.precision,
+                                      flags)
+        self.backends[0].handle.check(rc, "pb_batch_points")
+
+    def run(self):
+        """One step, eagerly: build every disc, interpolate all of them, wait and check."""
+        with self.torch.cuda.stream(self.stream):
+            self._enqueue(0)
+
+    def capture(self):
+        """Record one step (after an eager one has sized every buffer) in a CUDA graph."""
+        self.run()
+        g = self.torch.cuda.CUDAGraph()
+        with self.torch.cuda.graph(g, stream=self.stream):
+            self._enqueue(_lib.PB_BATCH_ASYNC)
+        self.graph = g
+        return g
+
+    def replay(self, check=True):
+        self.graph.replay()
+        if check:
+            self.backends[0].handle.check(self.lib.pb_batch_check(self.handles, self.K), "pb_batch_check")
+
+    def timed(self, steps=3, graph=True):
+        """Mean ms per step (CUDA events on the batch's stream) over `steps` steps."""
+        torch = self.torch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.stream.synchronize()
+        e0.record(self.stream)
+        for _ in range(steps):
+            if graph:
+                self.graph.replay()
+            else:
+                with torch.cuda.stream(self.stream):
+                    self._enqueue(_lib.PB_BATCH_ASYNC)
+        e1.record(self.stream)
+        e1.synchronize()
+        self.backends[0].handle.check(self.lib.pb_batch_check(self.handles, self.K), "pb_batch_check")
+        return e0.elapsed_time(e1) / steps
+
+    def outputs(self):
+        return [np.stack([o.cpu().numpy() for o in outs]) for outs in self.outs]
+
+    def close(self):
+        self.graph = None
+        for b in self.backends:
+            b.close()
+
+
+class BatchAutotuner:
+    """Schedule options of a DeviceBatch (outputs do not depend on them): every combination of
+    the candidates is captured and timed over `repeats` graph replays; the fastest is kept."""
+
+    def __init__(self, leaf_size=(1, 4, 8, 16), order=(0, 1), blocks_per_sm=(0, 2), repeats=2):
+        self.grid = {"leaf_size": leaf_size, "order": order, "blocks_per_sm": blocks_per_sm}
+        self.repeats = repeats
+        self.best = None
+        self.timings = []
+
+    def tune(self, batch):
+        best, best_ms = None, math.inf
+        for ls, od, bp in itertools.product(*self.grid.values()):
+            opts = {"leaf_size": ls, "order": od, "blocks_per_sm": bp}
+            batch.set_options(**opts)
+            batch.capture()
+            ms = batch.timed(self.repeats)
+            self.timings.append((opts, ms))
+            if ms < best_ms:
+                best, best_ms = opts, ms
+        batch.set_options(**best)
+        batch.capture()
+        self.best = best
+        return best

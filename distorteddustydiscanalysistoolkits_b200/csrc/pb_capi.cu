@@ -28,6 +28,10 @@ pb::Handle::~Handle()
                    &lpt_k, &lpt_v, &lpt_ka, &lpt_va, &iota, &grid_ax, &grid_out, &wl_cnt, &wl_off, &wl_s, &wl_j, &wl_sa, &wl_ja, &mlp_w, &mlp_m, &mlp_v, &mlp_g, &mlp_norm,
                    &mlp_scr, &mlp_idx, &mlp_x, &mlp_y, &mlp_loss, &sched_feat, &sched_pred, &sched_ql, &sched_tmp};
     for (DBuf *b : all) b->release();
+    batch_desc.release();
+    batch_starts.release();
+    batch_slots.release();
+    if (batch_host) cudaFreeHost(batch_host);
     for (auto &b : in_cols) b.release();
     for (auto &b : cols_s) b.release();
     for (auto &b : q_outs) b.release();
@@ -370,6 +374,8 @@ int query_order(Handle &H, int64_t nq, const double *dx, const double *dy, const
 int do_build(Handle &H, const pb_input *in, int32_t flags)
 {
     if (!in) return fail(H, PB_ERR_INVALID, "input is NULL");
+    if ((flags & PB_BUILD_ASYNC) && (flags & PB_PERMUTE_CALLER))
+        return fail(H, PB_ERR_INVALID, "PB_BUILD_ASYNC cannot permute the caller's arrays (that needs the sorted order)");
     int64_t n = in->npart;
     if (n < 1) return fail(H, PB_ERR_INVALID, "BinaryRadixTree: enc.codes must be non-empty (got n=0)");
     if (n > 1073741824LL) return fail(H, PB_ERR_CAPACITY, "n exceeds the Int32 node-id capacity (n <= 2^30)");
@@ -435,6 +441,12 @@ int do_build(Handle &H, const pb_input *in, int32_t flags)
     H.n = n;
     H.ncol = in->ncolumn;
     H.kernel = in->kernel;
+    if (flags & PB_BUILD_ASYNC) {
+        // no synchronisation: the status word is checked by a later synchronous call
+        // (pb_batch_check, or any query or interpolation entry point)
+        H.built = true;
+        return PB_OK;
+    }
     int rc = check_status(H);
     if (rc) return rc;
     H.t_build_ms = ev_ms(H, 0, 1);
@@ -923,6 +935,15 @@ int32_t pb_set_option(pb_handle *h, const char *name, int64_t value)
     } else if (!strcmp(name, "slice_queries")) {
         if (value < 1024) return fail(H, PB_ERR_INVALID, "slice_queries must be >= 1024");
         H.slice = value;
+    } else if (!strcmp(name, "leaf_size")) {
+        if (value < 1 || value > 64) return fail(H, PB_ERR_INVALID, "leaf_size must be in 1..64");
+        H.leaf_size = (int)value;
+    } else if (!strcmp(name, "batch_order")) {
+        if (value < 0 || value > 1) return fail(H, PB_ERR_INVALID, "batch_order must be 0 (given) or 1 (most work first)");
+        H.batch_order = (int)value;
+    } else if (!strcmp(name, "batch_blocks_per_sm")) {
+        if (value < 0 || value > 32) return fail(H, PB_ERR_INVALID, "batch_blocks_per_sm must be in 0..32");
+        H.batch_blocks = (int)value;
     } else if (!strcmp(name, "walk_split")) {
         if (value < 1 || value > 4096) return fail(H, PB_ERR_INVALID, "walk_split must be in 1..4096");
         H.walk_split = (int)value;
@@ -1398,6 +1419,136 @@ int32_t pb_last_schedule(const pb_handle *h, int64_t *walk_rounds, int64_t *defe
     if (deferred) *deferred = h->H.deferred_total;
     if (pool_chunks) *pool_chunks = (int64_t)h->H.pool_cap;
     return PB_OK;
+}
+
+namespace {
+
+int batch_fail(pb_handle *h, int code, const std::string &msg)
+{
+    if (h) h->H.err = msg;
+    return code;
+}
+
+int check_statuses(pb_handle *const *discs, int32_t ndiscs)
+{
+    Handle &H0 = discs[0]->H;
+    if (cudaStreamSynchronize(H0.stream) != cudaSuccess) {
+        cudaError_t e = cudaGetLastError();
+        return batch_fail(discs[0], PB_ERR_CUDA, std::string("batched launch: ") + cudaGetErrorString(e));
+    }
+    for (int32_t k = 0; k < ndiscs; ++k) {
+        int rc = check_status(discs[k]->H);
+        if (rc) return batch_fail(discs[0], rc, "disc " + std::to_string(k) + ": " + discs[k]->H.err);
+    }
+    return PB_OK;
+}
+
+}  // namespace
+
+int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalog *cat, const int64_t *npts,
+                        const double *const *qx, const double *const *qy, const double *const *qz, double *const *out,
+                        int32_t strategy, int32_t precision, int32_t flags)
+{
+    if (!discs || ndiscs < 1 || !discs[0]) return PB_ERR_INVALID;
+    pb_handle *h0 = discs[0];
+    Handle &H = h0->H;
+    if (ndiscs > 65536) return batch_fail(h0, PB_ERR_INVALID, "at most 65536 discs per batch");
+    if (strategy < 0 || strategy > 2) return batch_fail(h0, PB_ERR_INVALID, "unknown interpolation strategy");
+    if (precision != PB_FP64 && precision != PB_FP32C) return batch_fail(h0, PB_ERR_INVALID, "unknown precision mode");
+    if (!cat || !npts || !qx || !qy || !qz || !out) return batch_fail(h0, PB_ERR_INVALID, "NULL argument");
+    const int64_t L = catalog_L(cat);
+    if (L < 1) return batch_fail(h0, PB_ERR_INVALID, "empty catalog");
+    for (int32_t k = 0; k < ndiscs; ++k) {
+        if (!discs[k]) return batch_fail(h0, PB_ERR_INVALID, "NULL disc handle");
+        Handle &Hk = discs[k]->H;
+        if (!Hk.built) return batch_fail(h0, PB_ERR_STATE, "disc " + std::to_string(k) + " has no LBVH");
+        if (Hk.device != H.device || Hk.stream != H.stream)
+            return batch_fail(h0, PB_ERR_INVALID, "every disc handle must use the first one's device and stream");
+        if (Hk.kernel != H.kernel) return batch_fail(h0, PB_ERR_INVALID, "every disc must use the same kernel");
+        int rc = validate_catalog(Hk, cat, false);
+        if (rc) return batch_fail(h0, rc, "disc " + std::to_string(k) + ": " + Hk.err);
+        if (npts[k] < 0) return batch_fail(h0, PB_ERR_INVALID, "negative number of sample points");
+        if (npts[k] > 0 && (!is_device_ptr(H, qx[k]) || !is_device_ptr(H, qy[k]) || !is_device_ptr(H, qz[k])))
+            return batch_fail(h0, PB_ERR_INVALID, "batched sample points must be device memory of the handles' device");
+        for (int64_t l = 0; l < L; ++l)
+            if (npts[k] > 0 && !is_device_ptr(H, out[k * L + l]))
+                return batch_fail(h0, PB_ERR_INVALID, "batched outputs must be device memory of the handles' device");
+    }
+    const std::vector<Launch> p32 = plan(items_of(cat, true)), p64 = plan(items_of(cat, false));
+    if (p32.size() != 1 || p64.size() != 1)
+        return batch_fail(h0, PB_ERR_INVALID, "catalog needs more than one launch: not supported by the batched path");
+    CK(cudaSetDevice(H.device));
+    // processing order of the discs: given, or the most work (points x particles^(1/3)) first
+    std::vector<uint32_t> order(ndiscs);
+    for (int32_t k = 0; k < ndiscs; ++k) order[k] = (uint32_t)k;
+    if (H.batch_order == 1) {
+        std::vector<double> work(ndiscs);
+        for (int32_t k = 0; k < ndiscs; ++k) work[k] = (double)npts[k] * std::cbrt((double)discs[k]->H.n);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
+    }
+    // pinned staging: descriptors, starts (processing order) and slot -> disc
+    const size_t desc_bytes = sizeof(BatchDisc) * ndiscs, start_bytes = sizeof(int64_t) * (ndiscs + 1),
+                 slot_bytes = sizeof(uint32_t) * ndiscs;
+    const size_t host_bytes = desc_bytes + start_bytes + slot_bytes;
+    if (H.batch_host_bytes < host_bytes) {
+        if (H.batch_host) cudaFreeHost(H.batch_host);
+        H.batch_host = nullptr;
+        H.batch_host_bytes = 0;
+        CK(cudaMallocHost(&H.batch_host, host_bytes));
+        H.batch_host_bytes = host_bytes;
+    }
+    CK(H.batch_desc.reserve(desc_bytes));
+    CK(H.batch_starts.reserve(start_bytes));
+    CK(H.batch_slots.reserve(slot_bytes));
+    CK(H.counter.reserve(sizeof(unsigned long long)));
+    BatchDisc *hd = static_cast<BatchDisc *>(H.batch_host);
+    int64_t *hs = reinterpret_cast<int64_t *>(static_cast<char *>(H.batch_host) + desc_bytes);
+    uint32_t *ho = reinterpret_cast<uint32_t *>(static_cast<char *>(H.batch_host) + desc_bytes + start_bytes);
+    int64_t qtotal = 0;
+    for (int32_t i = 0; i < ndiscs; ++i) {
+        hs[i] = qtotal;
+        ho[i] = order[i];
+        qtotal += npts[order[i]];
+    }
+    hs[ndiscs] = qtotal;
+    for (int32_t k = 0; k < ndiscs; ++k) {
+        Handle &Hk = discs[k]->H;
+        BatchDisc D;
+        memset(&D, 0, sizeof(D));
+        D.T = make_tree(Hk);
+        D.C32 = dev_catalog(Hk, p32[0], out + k * L);
+        D.C64 = dev_catalog(Hk, p64[0], out + k * L);
+        D.qx = qx[k];
+        D.qy = qy[k];
+        D.qz = qz[k];
+        D.nq = npts[k];
+        if (precision == PB_FP32C) {
+            float4 *pay = nullptr;
+            int stride = 0;
+            CK(launch_batch_payload(&Hk, D.T, D.C32, &pay, &stride));
+            D.pay = pay;
+            D.stride = stride;
+        }
+        hd[k] = D;
+    }
+    CK(cudaMemcpyAsync(H.batch_desc.p, H.batch_host, desc_bytes, cudaMemcpyHostToDevice, H.stream));
+    CK(cudaMemcpyAsync(H.batch_starts.p, hs, start_bytes, cudaMemcpyHostToDevice, H.stream));
+    CK(cudaMemcpyAsync(H.batch_slots.p, ho, slot_bytes, cudaMemcpyHostToDevice, H.stream));
+    if (qtotal > 0)
+        CK(launch_batch_points(&H, strategy, H.kernel, H.batch_desc.as<BatchDisc>(), H.batch_starts.as<int64_t>(),
+                               H.batch_slots.as<uint32_t>(), ndiscs, qtotal, precision == PB_FP64 ? 1 : 0,
+                               (unsigned)H.light_max, H.leaf_size, H.batch_blocks,
+                               H.counter.as<unsigned long long>()));
+    if (flags & PB_BATCH_ASYNC) return PB_OK;
+    return check_statuses(discs, ndiscs);
+}
+
+int32_t pb_batch_check(pb_handle *const *discs, int32_t ndiscs)
+{
+    if (!discs || ndiscs < 1 || !discs[0]) return PB_ERR_INVALID;
+    for (int32_t k = 0; k < ndiscs; ++k)
+        if (!discs[k]) return batch_fail(discs[0], PB_ERR_INVALID, "NULL disc handle");
+    return check_statuses(discs, ndiscs);
 }
 
 int32_t pb_last_pair_split(const pb_handle *h, int64_t *heavy_queries, int64_t *light_queries, int64_t *heavy_pairs,

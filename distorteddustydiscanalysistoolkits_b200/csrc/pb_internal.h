@@ -10,6 +10,19 @@
 
 namespace pb {
 
+// One disc of a batched launch (pb_batch.cu): its tree, the FP32C and FP64 catalogs of its
+// columns and outputs, its FP32C payload, and its sample points.
+struct BatchDisc {
+    DevTree T;
+    DevCatalog C32, C64;
+    const float4 *pay;
+    const double *qx, *qy, *qz;
+    int64_t nq;
+    int stride;
+    int pad;
+};
+static_assert(sizeof(BatchDisc) % 8 == 0, "batch descriptors are copied in 8-byte words");
+
 // grow-only device buffer
 struct DBuf {
     void *p = nullptr;
@@ -91,6 +104,14 @@ struct Handle {
     // queries and accepted pairs of the last point call summed by the FP32C (heavy) and the
     // FP64 (light) pair kernels
     int64_t split_hq = 0, split_lq = 0, split_hp = 0, split_lp = 0;
+
+    // batched launch (pb_batch_points): descriptors, processing-order starts, pinned staging
+    DBuf batch_desc, batch_starts, batch_slots;
+    void *batch_host = nullptr;
+    size_t batch_host_bytes = 0;
+    int leaf_size = 1;       // warp-uniform walk: subtrees of at most this many leaves are scanned
+    int batch_order = 0;     // 0: discs in the given order, 1: discs with the most work first
+    int batch_blocks = 0;    // blocks per SM of the batched kernel (0: as many as fit)
 
     // query-side scratch
     DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
@@ -183,6 +204,10 @@ cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, 
 struct LineFrame {
     double c[3], e1[3], e2[3], d[3];
 };
+cudaError_t launch_batch_points(Handle *H, int strategy, int kernel, const BatchDisc *discs, const int64_t *starts,
+                                const uint32_t *slot_disc, int ndisc, int64_t qtotal, int fp64_only,
+                                unsigned light_max, int leaf_size, int blocks_per_sm, unsigned long long *ctr);
+cudaError_t launch_batch_payload(Handle *H, const DevTree &T, const DevCatalog &C, float4 **pay, int *stride);
 cudaError_t launch_line_image(Handle *H, const double *a0, int64_t n0, const double *a1, int64_t n1, const LineFrame &F,
                               double *ox, double *oy, double *oz, double *dx, double *dy, double *dz);
 

@@ -246,10 +246,13 @@ __device__ __forceinline__ bool node_pruned(const DevTree &T, const NodeF &nd, i
 
 // Warp-uniform form of the same walk for the warp-per-query kernels: returns the next
 // accepted item in DFS order, either a single leaf (lo == hi) or the whole contiguous leaf
-// range of a subtree that lies inside the query radius.
+// range of a subtree that lies inside the query radius.  With leaf_size > 1, a subtree of at
+// most leaf_size leaves that is neither pruned nor accepted whole is scanned leaf by leaf in
+// sorted order with the exact FP64 test instead of being descended: the accepted leaves and
+// their order -- hence every sum -- are the same, only the node visits change.
 template <int STRAT>
 __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, double py, double pz, double K,
-                                          double r2a, int64_t &lo, int64_t &hi)
+                                          double r2a, int64_t &lo, int64_t &hi, int leaf_size = 1)
 {
     const int64_t n = T.n;
     const QBox q = make_qbox(px, py, pz);
@@ -257,6 +260,20 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
     const float r2a_up = __double2float_ru(r2a);
     const float bulk_lim = __fmul_rd(__double2float_rd(r2a), MARGIN_DN);
     for (;;) {
+        if (w.cur <= w.end) {   // linear scan of a small subtree's leaves
+            if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.cur = 1; w.end = 0; w.node = w.stop; return false; }
+            const int64_t b = w.cur++;
+            const double4 L = ldg4(T.leaf + b);
+            double r2;
+            if (STRAT == GATHER) r2 = r2a;
+            else {
+                double r = __dmul_rn(K, L.w);
+                double rr = __dmul_rn(r, r);
+                r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+            }
+            if (d2_point(px, py, pz, L) <= r2) { lo = hi = b; return true; }
+            continue;
+        }
         if (w.node == w.stop) return false;
         if (++w.guard > w.limit) { flag(T.status, ST_TRAVERSAL); w.node = w.stop; return false; }
         const int node = w.node;
@@ -282,6 +299,15 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
             hi = rg.y;
             w.node = nd.escape;
             return true;
+        }
+        if (leaf_size > 1) {
+            const int2 rg = __ldg(T.range + (node - 1));
+            if (rg.y - rg.x < leaf_size) {   // scan this subtree's leaves, then continue after it
+                w.cur = rg.x;
+                w.end = rg.y;
+                w.node = nd.escape;
+                continue;
+            }
         }
         w.node = nd.left;
     }

@@ -50,6 +50,10 @@ extern "C" {
 
 /* flags for pb_linear_bvh / pb_*_samples_interpolation */
 #define PB_PERMUTE_CALLER 1   /* permute the caller's particle arrays in place, as LinearBVH! does */
+#define PB_BUILD_ASYNC 2      /* pb_linear_bvh: enqueue the build without waiting for it; its status is
+                                 checked by the next synchronous call on the handle or pb_batch_check */
+/* flags for pb_batch_points */
+#define PB_BATCH_ASYNC 1      /* enqueue only; pb_batch_check waits and checks every disc's status */
 
 typedef struct pb_handle pb_handle;
 
@@ -163,6 +167,25 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
                                       const double *ox, const double *oy, const double *oz, const double *dx,
                                       const double *dy, const double *dz, int32_t strategy, int32_t precision,
                                       double *const *out, int32_t flags);
+
+/* Batched PointSamples interpolation over many snapshots (the reference interpolates one
+   snapshot per call, PointSamples_interpolation.jl:12-29; this batches calls).  discs[k] is a
+   handle on which pb_linear_bvh has built disc k (PB_BUILD_ASYNC allowed); npts[k] sample
+   points at qx[k], qy[k], qz[k] and the L = n_scalar + 3 n_grad + n_div + 3 n_curl outputs
+   out[k * L + l] are device memory.  One persistent kernel sums every disc's points (FP64: the
+   reference's arithmetic; FP32C: queries with at most fp64_light_max neighbours in FP64, the
+   rest FP32-compensated, decided on the device), with values equal to separate
+   pb_interpolate_points calls bit for bit.  Every handle must use the first one's device,
+   stream (pb_set_stream) and kernel; the catalog must fit one launch.  Options of discs[0]:
+   "leaf_size" (walk cutoff), "batch_order" (0 given, 1 most work first) and
+   "batch_blocks_per_sm" (0 = all that fit) change the schedule only.  With device pointers, no
+   synchronisation and all buffers already sized by an earlier identical call, the builds with
+   PB_BUILD_ASYNC and this call with PB_BATCH_ASYNC can be captured in a CUDA graph. */
+int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalog *cat, const int64_t *npts,
+                        const double *const *qx, const double *const *qy, const double *const *qz, double *const *out,
+                        int32_t strategy, int32_t precision, int32_t flags);
+/* Wait for the batch's stream and check every disc's device status word (build and traversal). */
+int32_t pb_batch_check(pb_handle *const *discs, int32_t ndiscs);
 
 /* Morton encode + stable radix sort + duplicate bump of the LBVH build (the sorted
    MortonEncoding codes and the 0-based sorting order) without allocating any device memory.
