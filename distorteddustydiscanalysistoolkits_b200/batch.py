@@ -202,7 +202,8 @@ class DeviceBatch:
         return g
 
     def replay(self, check=True):
-        self.graph.replay()
+        with self.torch.cuda.stream(self.stream):   # a graph replays on the current stream
+            self.graph.replay()
         if check:
             self.backends[0].handle.check(self.lib.pb_batch_check(self.handles, self.K), "pb_batch_check")
 
@@ -211,14 +212,14 @@ class DeviceBatch:
         torch = self.torch
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         self.stream.synchronize()
-        e0.record(self.stream)
-        for _ in range(steps):
-            if graph:
-                self.graph.replay()
-            else:
-                with torch.cuda.stream(self.stream):
+        with torch.cuda.stream(self.stream):   # the graph replays on the current stream
+            e0.record(self.stream)
+            for _ in range(steps):
+                if graph:
+                    self.graph.replay()
+                else:
                     self._enqueue(_lib.PB_BATCH_ASYNC)
-        e1.record(self.stream)
+            e1.record(self.stream)
         e1.synchronize()
         self.backends[0].handle.check(self.lib.pb_batch_check(self.handles, self.K), "pb_batch_check")
         return e0.elapsed_time(e1) / steps

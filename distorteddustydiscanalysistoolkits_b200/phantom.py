@@ -292,7 +292,7 @@ def build_input_device(df, mass_from, backend, scalars=(), gradients=(), diverge
     from ._lib import ptr
     names = _quantity_columns(scalars, gradients, divergences, curls)
     if rho_from_h:
-        need = [k for k in ("x", "y", "z", "h") if k not in df] + [k for k in names if k not in df]
+        need = [k for k in ("x", "y", "z", "h") if k not in df] + [k for k in names if k not in df and k != "rho"]
         if need:
             raise ArgumentError("Missing columns in ParticleDataFrame: " + ", ".join(need))
         if df.params.get("mass") is None:
@@ -325,6 +325,9 @@ def build_input_device(df, mass_from, backend, scalars=(), gradients=(), diverge
                                         rho.data_ptr()), "build_input_device")
     else:
         rho = upload(df["rho"])
-    inp = InterpolationInput(x, y, z, m, h, rho, tuple(upload(df[k]) for k in names), smoothed_kernel=smoothed_kernel)
+    # a "rho" quantity column is the density itself (derived from h when rho_from_h, as add_rho!
+    # followed by build_input gives it)
+    quant = tuple(rho.clone() if (k == "rho" and rho_from_h) else upload(df[k]) for k in names)
+    inp = InterpolationInput(x, y, z, m, h, rho, quant, smoothed_kernel=smoothed_kernel)
     cat = InterpolationCatalog(names, scalars=scalars, gradients=gradients, divergences=divergences, curls=curls)
     return inp, cat
