@@ -34,7 +34,7 @@ UNITS = {
     "pb_input.cu": ["-fmad=false"],
     "pb_batch.cu": ["-fmad=false"],
 }
-HEADERS = ["pb_device.cuh", "pb_internal.h", "pb_interp_impl.cuh", "pb_fp32_impl.cuh", "pb_fp64_impl.cuh",
+HEADERS = ["pb_device.cuh", "pb_internal.h", "pb_interp_impl.cuh", "pb_fp32_impl.cuh", "pb_fp64_impl.cuh", "pb_walk_impl.cuh",
            "line_tables.h"]
 
 

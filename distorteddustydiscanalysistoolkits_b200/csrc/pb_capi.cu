@@ -672,6 +672,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
             P.deferred = lists[round & 1];
             P.count_only = 0;
+            P.leaf_size = H.leaf_size;
             ev_record(H, 4);
             if (strategy != SCATTER || mode == 2) {
                 CK(launch_nearest_list(&H, T, m, ql, dx, dy, dz, P.bnear));
@@ -1489,7 +1490,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
     // pinned staging: descriptors, starts (processing order) and slot -> disc
     const size_t desc_bytes = sizeof(BatchDisc) * ndiscs, start_bytes = sizeof(int64_t) * (ndiscs + 1),
                  slot_bytes = sizeof(uint32_t) * ndiscs;
-    const size_t host_bytes = desc_bytes + start_bytes + slot_bytes;
+    const size_t host_bytes = desc_bytes + start_bytes + slot_bytes + sizeof(int2);
     if (H.batch_host_bytes < host_bytes) {
         if (H.batch_host) cudaFreeHost(H.batch_host);
         H.batch_host = nullptr;
@@ -1534,11 +1535,47 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
     CK(cudaMemcpyAsync(H.batch_desc.p, H.batch_host, desc_bytes, cudaMemcpyHostToDevice, H.stream));
     CK(cudaMemcpyAsync(H.batch_starts.p, hs, start_bytes, cudaMemcpyHostToDevice, H.stream));
     CK(cudaMemcpyAsync(H.batch_slots.p, ho, slot_bytes, cudaMemcpyHostToDevice, H.stream));
-    if (qtotal > 0)
-        CK(launch_batch_points(&H, strategy, H.kernel, H.batch_desc.as<BatchDisc>(), H.batch_starts.as<int64_t>(),
-                               H.batch_slots.as<uint32_t>(), ndiscs, qtotal, precision == PB_FP64 ? 1 : 0,
-                               (unsigned)H.light_max, H.leaf_size, H.batch_blocks,
-                               H.counter.as<unsigned long long>()));
+    // slices of a fixed size share one run pool, sized once (a call that reuses it allocates
+    // nothing, which is what lets a step be captured in a CUDA graph)
+    const int64_t S = std::max<int64_t>(1, std::min<int64_t>(H.slice > 0 ? H.slice : qtotal, qtotal));
+    if (qtotal > 0 && (H.pool_cap == 0 || H.batch_slice < S)) {
+        int rc = reserve_pool(H, S, 1);
+        if (rc) return rc;
+        H.batch_slice = S;
+    }
+    if (qtotal > 0) {
+        // the cut of a batch: every tree whole (root 1, stop 0), staged in pinned memory
+        int2 *hcut = reinterpret_cast<int2 *>(static_cast<char *>(H.batch_host) + desc_bytes + start_bytes + slot_bytes);
+        *hcut = make_int2(1, 0);
+        CK(H.cut.reserve(sizeof(int2)));
+        CK(cudaMemcpyAsync(H.cut.p, hcut, sizeof(int2), cudaMemcpyHostToDevice, H.stream));
+        unsigned long long *ctr = H.pool_ctr.as<unsigned long long>();
+        RunPool P;
+        P.runs = H.pool_runs.as<uint2>();
+        P.next = H.pool_next.as<int>();
+        P.used = ctr;
+        P.cap = H.pool_cap;
+        P.ns = 1;
+        P.cut = H.cut.as<int2>();
+        P.items = H.items.as<int2>();
+        P.bnear = H.wbnear.as<int>();
+        P.qacc = H.qacc.as<unsigned>();
+        P.qflag = H.qflag.as<int>();
+        P.n_deferred = reinterpret_cast<unsigned *>(ctr + 1);
+        P.deferred = H.defer_a.as<uint32_t>();
+        P.count_only = 0;
+        P.leaf_size = H.leaf_size;
+        for (int64_t s0 = 0; s0 < qtotal; s0 += S) {
+            const int64_t m = std::min<int64_t>(S, qtotal - s0);
+            CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
+            CK(cudaMemsetAsync(P.qacc, 0, sizeof(unsigned) * m, H.stream));
+            CK(cudaMemsetAsync(P.qflag, 0, sizeof(int) * m, H.stream));
+            CK(launch_batch_slice(&H, strategy, H.kernel, H.batch_desc.as<BatchDisc>(), H.batch_starts.as<int64_t>(),
+                                  H.batch_slots.as<uint32_t>(), ndiscs, s0, m, P, precision == PB_FP64 ? 1 : 0,
+                                  (unsigned)H.light_max, H.leaf_size, H.batch_blocks,
+                                  H.counter.as<unsigned long long>()));
+        }
+    }
     if (flags & PB_BATCH_ASYNC) return PB_OK;
     return check_statuses(discs, ndiscs);
 }

@@ -80,6 +80,7 @@ struct RunPool {
     unsigned *n_deferred;         // queries deferred in this walk
     uint32_t *deferred;           // their query indices
     int count_only;               // 1: only count accepted leaves (qacc); no runs, no items
+    int leaf_size;                // walk cutoff: subtrees of at most this many leaves are scanned
 };
 
 // Catalog of one launch.  ucol[] are the unique sorted quantity columns read per

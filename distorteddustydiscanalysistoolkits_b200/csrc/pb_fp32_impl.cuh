@@ -497,4 +497,53 @@ __device__ __forceinline__ void points32_query(const DevTree &T, const DevCatalo
     reduce_finalize32<CAT_ANY>(A, C, qi, lane);
 }
 
+
+// The two-phase FP32-compensated sum of one walked query j (its runs in the pool P) at sample
+// point qi: the k-th accepted leaf to lane k mod 32, in DFS order, exactly as the fused body
+// deals them, so both give the same bits.  Every lane of the warp calls it.
+template <int STRAT, int KT, int CAT>
+__device__ __forceinline__ void pairs32_query(const DevTree &T, const DevCatalog &C, const float4 *__restrict__ pay,
+                                              int stride, const RunPool &P, int64_t j, int64_t qi, double px,
+                                              double py, double pz, int64_t bnear, double *s_acc, int lane)
+{
+    const float sig = ldexp_norm3(KT);
+    Query32 Q;
+    Acc32 A;
+    setup32<STRAT, CAT>(T, sig, px, py, pz, bnear, Q, A, pay, stride, s_acc + threadIdx.x);
+    int nb = 0;   // full batches since the last flush (warp-uniform)
+    int mine = -1;
+    auto first = [&](int b0) {
+        if (!A.have) offsets_from<CAT>(A, pay, stride, b0);
+    };
+    auto one = [&](int b) {
+        pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, b);
+        if (++nb == CHUNK) {
+            A.flush<CAT>(C);
+            nb = 0;
+        }
+    };
+    auto two = [&](int m1) {   // flush boundary after the second batch (nb is even here)
+        pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
+        nb += 2;
+        if (nb == CHUNK) {
+            A.flush<CAT>(C);
+            nb = 0;
+        }
+    };
+    auto four = [&](int m1) {   // flush boundary after the fourth batch (nb is a multiple of 4 here)
+        pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
+        pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1 + 64, m1 + 96);
+        nb += 4;
+        if (nb == CHUNK) {
+            A.flush<CAT>(C);
+            nb = 0;
+        }
+    };
+    auto cantwo = [&]() { return (nb & 1) == 0; };
+    auto canfour = [&]() { return (nb & 3) == 0; };
+    deal_runs(P, j, lane, first, one, two, cantwo, four, canfour, mine);
+    if (mine >= 0) pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, mine);
+    reduce_finalize32<CAT>(A, C, qi, lane);
+}
+
 }  // namespace pb

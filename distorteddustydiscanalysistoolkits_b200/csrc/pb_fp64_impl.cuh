@@ -136,4 +136,46 @@ __device__ __forceinline__ void points64_query(const DevTree &T, const DevCatalo
     if (lane == 0) finalize64(v, C, qi);
 }
 
+// The two-phase FP64 sum of one walked query j (its runs in the pool P) at sample point qi:
+// the accepted leaves dealt in DFS order, the terms and in-order sums of points64_query.
+template <int STRAT>
+__device__ __forceinline__ void pairs64_query(const DevTree &T, const DevCatalog &C, const RunPool &P, int64_t j,
+                                              int64_t qi, double px, double py, double pz, int64_t bnear,
+                                              double *sterm, int lane)
+{
+    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
+    double ha = 0.0;
+    if (STRAT != SCATTER) ha = bnear < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + bnear).w;
+    double acc = 0.0;   // lane a < NT owns accumulator a
+    auto proc = [&](int fill, int64_t b) {
+        if (b >= 0) {
+            double tv[NT];
+            terms64<STRAT>(T, C, need_grad, px, py, pz, b, ha, tv);
+#pragma unroll
+            for (int a = 0; a < NT; ++a) sterm[lane * (NT + 1) + a] = tv[a];
+        }
+        __syncwarp();
+        if (lane < NT)
+            for (int s = 0; s < fill; ++s) acc += sterm[s * (NT + 1) + lane];
+        __syncwarp();
+    };
+    auto first = [&](int64_t) {};
+    auto one = [&](int64_t b) { proc(32, b); };
+    auto two = [&](int64_t m1) {
+        proc(32, m1);
+        proc(32, m1 + 32);
+    };
+    auto cantwo = [&]() { return false; };
+    // never called (canfour is false): an empty body keeps the kernels free of a stack frame,
+    // which a four-batch body here would force on the per-pair term array
+    auto four = [&](int64_t) {};
+    int mine = -1;
+    const int fill = deal_runs(P, j, lane, first, one, two, cantwo, four, cantwo, mine);
+    if (fill > 0) proc(fill, mine);
+    double v[NT];
+#pragma unroll
+    for (int a = 0; a < NT; ++a) v[a] = __shfl_sync(0xffffffffu, acc, a);
+    if (lane == 0) finalize64(v, C, qi);
+}
+
 }  // namespace pb

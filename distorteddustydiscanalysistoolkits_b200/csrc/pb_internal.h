@@ -111,7 +111,8 @@ struct Handle {
     size_t batch_host_bytes = 0;
     int leaf_size = 1;       // warp-uniform walk: subtrees of at most this many leaves are scanned
     int batch_order = 0;     // 0: discs in the given order, 1: discs with the most work first
-    int batch_blocks = 0;    // blocks per SM of the batched kernel (0: as many as fit)
+    int batch_blocks = 0;    // blocks per SM of the batched pair kernel (0: as many as fit)
+    int64_t batch_slice = 0; // sample points per slice the batch's run pool was sized for
 
     // query-side scratch
     DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
@@ -204,9 +205,10 @@ cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, 
 struct LineFrame {
     double c[3], e1[3], e2[3], d[3];
 };
-cudaError_t launch_batch_points(Handle *H, int strategy, int kernel, const BatchDisc *discs, const int64_t *starts,
-                                const uint32_t *slot_disc, int ndisc, int64_t qtotal, int fp64_only,
-                                unsigned light_max, int leaf_size, int blocks_per_sm, unsigned long long *ctr);
+cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, const BatchDisc *discs, const int64_t *starts,
+                               const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m, const RunPool &P,
+                               int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
+                               unsigned long long *ctr);
 cudaError_t launch_batch_payload(Handle *H, const DevTree &T, const DevCatalog &C, float4 **pay, int *stride);
 cudaError_t launch_line_image(Handle *H, const double *a0, int64_t n0, const double *a1, int64_t n1, const LineFrame &F,
                               double *ox, double *oy, double *oz, double *dx, double *dy, double *dz);

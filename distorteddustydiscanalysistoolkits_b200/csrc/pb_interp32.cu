@@ -61,7 +61,6 @@ __global__ void __launch_bounds__(128, 5) k_pairs32w(DevTree T, DevCatalog C, co
 {
     __shared__ double s_acc[ACC_SLOTS * ACC_STRIDE];   // FP64 sums, slot k of thread t at [k * 128 + t]
     const int lane = threadIdx.x & 31;
-    const float sig = ldexp_norm3(KT);
     for (;;) {
         int64_t t = next_query(counter, lane);
         if (t >= m) break;
@@ -69,44 +68,8 @@ __global__ void __launch_bounds__(128, 5) k_pairs32w(DevTree T, DevCatalog C, co
         if (__ldg(P.qflag + j)) continue;
         const int64_t qi = __ldg(ql + j);
         const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
-        Query32 Q;
-        Acc32 A;
-        setup32<STRAT, CAT>(T, sig, px, py, pz, STRAT != SCATTER ? __ldg(P.bnear + j) : -1, Q, A, pay, stride,
-                            s_acc + threadIdx.x);
-        int nb = 0;   // full batches since the last flush (warp-uniform)
-        int mine = -1;
-        auto first = [&](int b0) {
-            if (!A.have) offsets_from<CAT>(A, pay, stride, b0);
-        };
-        auto one = [&](int b) {
-            pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, b);
-            if (++nb == CHUNK) {
-                A.flush<CAT>(C);
-                nb = 0;
-            }
-        };
-        auto two = [&](int m1) {   // flush boundary after the second batch (nb is even here)
-            pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
-            nb += 2;
-            if (nb == CHUNK) {
-                A.flush<CAT>(C);
-                nb = 0;
-            }
-        };
-        auto four = [&](int m1) {   // flush boundary after the fourth batch (nb is a multiple of 4 here)
-            pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
-            pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1 + 64, m1 + 96);
-            nb += 4;
-            if (nb == CHUNK) {
-                A.flush<CAT>(C);
-                nb = 0;
-            }
-        };
-        auto cantwo = [&]() { return (nb & 1) == 0; };
-        auto canfour = [&]() { return (nb & 3) == 0; };
-        deal_runs(P, j, lane, first, one, two, cantwo, four, canfour, mine);
-        if (mine >= 0) pair32<STRAT, KT, CAT>(A, C, Q, pay, stride, mine);
-        reduce_finalize32<CAT>(A, C, qi, lane);
+        pairs32_query<STRAT, KT, CAT>(T, C, pay, stride, P, j, qi, px, py, pz,
+                                      STRAT != SCATTER ? (int64_t)__ldg(P.bnear + j) : -1, s_acc, lane);
     }
 }
 

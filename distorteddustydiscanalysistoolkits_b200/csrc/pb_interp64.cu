@@ -40,7 +40,6 @@ __global__ void __launch_bounds__(128) k_pairs64w(DevTree T, DevCatalog C, RunPo
 {
     __shared__ double sterm[4][32][NT + 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const bool need_grad = (C.n_grad + C.n_div + C.n_curl) > 0;
     for (;;) {
         int64_t t = next_query(counter, lane);
         if (t >= m) break;
@@ -48,41 +47,8 @@ __global__ void __launch_bounds__(128) k_pairs64w(DevTree T, DevCatalog C, RunPo
         if (__ldg(P.qflag + j)) continue;
         const int64_t qi = __ldg(ql + j);
         const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
-        double ha = 0.0;
-        if (STRAT != SCATTER) {
-            const int b = __ldg(P.bnear + j);
-            ha = b < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + b).w;
-        }
-        double acc = 0.0;   // lane a < NT owns accumulator a
-        auto proc = [&](int fill, int64_t b) {
-            if (b >= 0) {
-                double tv[NT];
-                terms64<STRAT>(T, C, need_grad, px, py, pz, b, ha, tv);
-#pragma unroll
-                for (int a = 0; a < NT; ++a) sterm[wib][lane][a] = tv[a];
-            }
-            __syncwarp();
-            if (lane < NT)
-                for (int s = 0; s < fill; ++s) acc += sterm[wib][s][lane];
-            __syncwarp();
-        };
-        auto first = [&](int64_t) {};
-        auto one = [&](int64_t b) { proc(32, b); };
-        auto two = [&](int64_t m1) {
-            proc(32, m1);
-            proc(32, m1 + 32);
-        };
-        auto cantwo = [&]() { return false; };
-        // never called (canfour is false): an empty body keeps this kernel free of a stack
-        // frame, which a four-batch body here would force on the per-pair term array
-        auto four = [&](int64_t) {};
-        int mine = -1;
-        const int fill = deal_runs(P, j, lane, first, one, two, cantwo, four, cantwo, mine);
-        if (fill > 0) proc(fill, mine);
-        double v[NT];
-#pragma unroll
-        for (int a = 0; a < NT; ++a) v[a] = __shfl_sync(0xffffffffu, acc, a);
-        if (lane == 0) finalize64(v, C, qi);
+        pairs64_query<STRAT>(T, C, P, j, qi, px, py, pz, STRAT != SCATTER ? (int64_t)__ldg(P.bnear + j) : -1,
+                             &sterm[wib][0][0], lane);
     }
 }
 

@@ -316,11 +316,12 @@ __device__ __forceinline__ bool next_item(const DevTree &T, Walk &w, double px, 
 // Flat form of the same walk for one thread, over the subtree entered at `start` and left at
 // `stop`: one node step per loop iteration, and every accepted item (a single leaf, or the
 // whole leaf range of a subtree inside the query radius) passed to emit(lo, hi) in DFS order.
-// The decisions are next_item's, step for step; a warp running this loop reconverges once
-// per node step instead of once per accepted item.  Returns false if emit refused an item.
+// The decisions are next_item's, step for step (with the same leaf_size cutoff: a small
+// subtree's leaves tested in sorted order); a warp running this loop reconverges once per node
+// step instead of once per accepted item.  Returns false if emit refused an item.
 template <int STRAT, typename EMIT>
 __device__ __forceinline__ bool walk_subtree(const DevTree &T, int start, int stop, double px, double py, double pz,
-                                             double K, double r2a, EMIT &emit)
+                                             double K, double r2a, EMIT &emit, int leaf_size = 1)
 {
     const int64_t n = T.n;
     const QBox q = make_qbox(px, py, pz);
@@ -356,6 +357,24 @@ __device__ __forceinline__ bool walk_subtree(const DevTree &T, int start, int st
                 const int2 rg = __ldg(T.range + (node - 1));
                 lo = rg.x;
                 hi = rg.y;
+                node = nd.escape;
+            } else if (leaf_size > 1 && __ldg(&T.range[node - 1].y) - __ldg(&T.range[node - 1].x) < leaf_size) {
+                const int2 rg = __ldg(T.range + (node - 1));
+                for (int64_t b = rg.x; b <= rg.y; ++b) {   // the subtree's leaves in sorted order
+                    if (++guard > limit) {
+                        flag(T.status, ST_TRAVERSAL);
+                        return true;
+                    }
+                    const double4 L = ldg4(T.leaf + b);
+                    double r2;
+                    if (STRAT == GATHER) r2 = r2a;
+                    else {
+                        const double r = __dmul_rn(K, L.w);
+                        const double rr = __dmul_rn(r, r);
+                        r2 = STRAT == SCATTER ? rr : (r2a > rr ? r2a : rr);
+                    }
+                    if (d2_point(px, py, pz, L) <= r2 && !emit(b, b)) return false;
+                }
                 node = nd.escape;
             } else {
                 node = nd.left;

@@ -45,7 +45,7 @@ def test_build_input_device_matches_host(backend, tmp_path):
         assert np.array_equal(a.cpu().numpy(), b)
     # mass from a float32 column, widened on the device
     df["mcol"] = np.full(df.npart, 2e-6, np.float32)
-    d2, _ = phantom.build_input_device(df, phantom.MassFromColumn("mcol"), backend, scalars=("vz",))
+    d2, _ = phantom.build_input_device(df, phantom.MassFromColumn("mcol"), backend, scalars=("vz",), rho_from_h=True)
     assert np.array_equal(d2.m.cpu().numpy(), df["mcol"].astype(np.float64))
     # the same interpolation from either input; FP64 equals the oracle bit for bit
     flat = pb.flatten(pb.Cartesian, synthetic.cartesian_box_grid(
