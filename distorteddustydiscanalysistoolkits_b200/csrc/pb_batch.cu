@@ -73,74 +73,157 @@ __global__ void __launch_bounds__(128) k_batch_walk(const BatchDisc *__restrict_
     }
 }
 
+// sort keys of a slice's pair order: 0x7fffffff - accepted (heaviest first); overflowed last
+__global__ void k_batch_keys(int64_t m, const unsigned *__restrict__ qacc, const int *__restrict__ qflag,
+                             uint32_t *keys, uint32_t *vals)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned a = qacc[t];
+        keys[t] = qflag[t] ? 0x80000000u : 0x7fffffffu - (a > 0x7fffffffu ? 0x7fffffffu : a);
+        vals[t] = (uint32_t)t;
+    }
+}
+
+// Per-warp copy of the descriptor of the disc of global point j (warp-uniform).
+struct DescCache {
+    int cur = -1;
+    __device__ __forceinline__ const BatchDisc &get(const BatchDisc *__restrict__ discs, BatchDisc &slot, int k, int lane)
+    {
+        if (k != cur) {
+            __syncwarp();
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(discs + k);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&slot);
+            for (int w = lane; w < (int)(sizeof(BatchDisc) / 8); w += 32) dst[w] = __ldg(src + w);
+            __syncwarp();
+            cur = k;
+        }
+        return slot;
+    }
+};
+
+// the slice's points in pair order (heaviest first, overflowed last): positions [0, nheavy)
+// are FP32C points, [nheavy, m - nover) FP64 points, [m - nover, m) points whose runs did not
+// fit the pool; ord[t] is the slice-local point
+struct SliceOrder {
+    const uint32_t *ord;
+    const unsigned *nheavy;      // device counters of the slice
+    const unsigned *nover;
+};
+
+template <int STRAT, int KT, int CAT>
+__global__ void __launch_bounds__(128, 5) k_batch_pairs32(const BatchDisc *__restrict__ discs,
+                                                          const int64_t *__restrict__ starts,
+                                                          const uint32_t *__restrict__ slot_disc, int ndisc, int64_t s0,
+                                                          RunPool P, SliceOrder O, unsigned long long *counter)
+{
+    __shared__ double s_acc[ACC_SLOTS * ACC_STRIDE];
+    __shared__ BatchDisc s_desc[BATCH_WARPS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t end = *O.nheavy;
+    DescCache dc;
+    for (;;) {
+        const int64_t pos = next_query(counter, lane);
+        if (pos >= end) break;
+        const int64_t t = __ldg(O.ord + pos), j = s0 + t;
+        const int lo = batch_slot(starts, ndisc, j);
+        const BatchDisc &D = dc.get(discs, s_desc[wib], (int)__ldg(slot_disc + lo), lane);
+        const DevTree T = D.T;
+        const int64_t qi = j - __ldg(starts + lo);
+        const double px = __ldg(D.qx + qi), py = __ldg(D.qy + qi), pz = __ldg(D.qz + qi);
+        pairs32_query<STRAT, KT, CAT>(T, D.C32, D.pay, D.stride, P, t, qi, px, py, pz,
+                                      STRAT != SCATTER ? (int64_t)__ldg(P.bnear + t) : -1, s_acc, lane);
+    }
+}
+
+template <int STRAT>
+__global__ void __launch_bounds__(128) k_batch_pairs64(const BatchDisc *__restrict__ discs,
+                                                       const int64_t *__restrict__ starts,
+                                                       const uint32_t *__restrict__ slot_disc, int ndisc, int64_t s0,
+                                                       int64_t m, RunPool P, SliceOrder O, unsigned long long *counter)
+{
+    __shared__ double s_term[BATCH_WARPS][32 * (NT + 1)];
+    __shared__ BatchDisc s_desc[BATCH_WARPS];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t first = *O.nheavy, end = m - (int64_t)*O.nover;
+    DescCache dc;
+    for (;;) {
+        const int64_t pos = first + next_query(counter, lane);
+        if (pos >= end) break;
+        const int64_t t = __ldg(O.ord + pos), j = s0 + t;
+        const int lo = batch_slot(starts, ndisc, j);
+        const BatchDisc &D = dc.get(discs, s_desc[wib], (int)__ldg(slot_disc + lo), lane);
+        const DevTree T = D.T;
+        const int64_t qi = j - __ldg(starts + lo);
+        const double px = __ldg(D.qx + qi), py = __ldg(D.qy + qi), pz = __ldg(D.qz + qi);
+        pairs64_query<STRAT>(T, D.C64, P, t, qi, px, py, pz, STRAT != SCATTER ? (int64_t)__ldg(P.bnear + t) : -1,
+                             s_term[wib], lane);
+    }
+}
+
+// points whose runs did not fit the pool: the fused walk-and-sum bodies, routed by a counting walk
 template <int STRAT, int KT>
-__global__ void __launch_bounds__(128) k_batch_pairs(const BatchDisc *__restrict__ discs,
-                                                     const int64_t *__restrict__ starts,
-                                                     const uint32_t *__restrict__ slot_disc, int ndisc, int64_t s0,
-                                                     int64_t m, RunPool P, int fp64_only, unsigned light_max,
-                                                     int leaf_size, unsigned long long *counter)
+__global__ void __launch_bounds__(128) k_batch_over(const BatchDisc *__restrict__ discs,
+                                                    const int64_t *__restrict__ starts,
+                                                    const uint32_t *__restrict__ slot_disc, int ndisc, int64_t s0,
+                                                    int64_t m, RunPool P, SliceOrder O, int fp64_only,
+                                                    unsigned light_max, int leaf_size, unsigned long long *counter)
 {
     __shared__ double s_acc[ACC_SLOTS * ACC_STRIDE];
     __shared__ double s_term[BATCH_WARPS][32 * (NT + 1)];
     __shared__ BatchDisc s_desc[BATCH_WARPS];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int cur = -1;   // disc whose descriptor this warp's slot holds
+    const int64_t first = m - (int64_t)*O.nover;
+    DescCache dc;
     for (;;) {
-        const int64_t t = next_query(counter, lane);
-        if (t >= m) break;
-        const int64_t j = s0 + t;
+        const int64_t pos = first + next_query(counter, lane);
+        if (pos >= m) break;
+        const int64_t t = __ldg(O.ord + pos), j = s0 + t;
         const int lo = batch_slot(starts, ndisc, j);
-        const int k = (int)__ldg(slot_disc + lo);
-        if (k != cur) {   // warp-uniform: copy the disc's descriptor into the warp's slot
-            __syncwarp();
-            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(discs + k);
-            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_desc[wib]);
-            for (int w = lane; w < (int)(sizeof(BatchDisc) / 8); w += 32) dst[w] = __ldg(src + w);
-            __syncwarp();
-            cur = k;
-        }
-        const BatchDisc &D = s_desc[wib];
+        const BatchDisc &D = dc.get(discs, s_desc[wib], (int)__ldg(slot_disc + lo), lane);
         const DevTree T = D.T;
         const int64_t qi = j - __ldg(starts + lo);
         const double px = __ldg(D.qx + qi), py = __ldg(D.qy + qi), pz = __ldg(D.qz + qi);
         const int64_t bnear = STRAT != SCATTER ? (int64_t)__ldg(P.bnear + t) : -1;
-        if (__ldg(P.qflag + t)) {   // runs did not fit the pool: the fused bodies walk again
-            const bool fp64 = fp64_only || count_accepted<STRAT>(T, px, py, pz, bnear, leaf_size) <= (int64_t)light_max;
-            if (fp64) points64_query<STRAT>(T, D.C64, px, py, pz, bnear, qi, s_term[wib], lane, leaf_size);
-            else points32_query<STRAT, KT>(T, D.C32, D.pay, D.stride, px, py, pz, bnear, qi, s_acc, lane, leaf_size);
-        } else if (fp64_only || __ldg(P.qacc + t) <= light_max) {
-            pairs64_query<STRAT>(T, D.C64, P, t, qi, px, py, pz, bnear, s_term[wib], lane);
-        } else {
-            pairs32_query<STRAT, KT, CAT_ANY>(T, D.C32, D.pay, D.stride, P, t, qi, px, py, pz, bnear, s_acc, lane);
+        const bool fp64 = fp64_only || count_accepted<STRAT>(T, px, py, pz, bnear, leaf_size) <= (int64_t)light_max;
+        if (fp64) points64_query<STRAT>(T, D.C64, px, py, pz, bnear, qi, s_term[wib], lane, leaf_size);
+        else points32_query<STRAT, KT>(T, D.C32, D.pay, D.stride, px, py, pz, bnear, qi, s_acc, lane, leaf_size);
+    }
+}
+
+template <typename KERN>
+static int persistent_blocks_of(KERN kern, int cap)
+{
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)kern, 128, 0);
+    if (per < 1) per = 1;
+    if (cap > 0 && cap < per) per = cap;
+    return sms * per;
+}
+
+template <int STRAT, int KT>
+static void launch_slice_pairs(Handle *H, int cat, const BatchDisc *discs, const int64_t *starts, const uint32_t *slot_disc,
+                               int ndisc, int64_t s0, int64_t m, const RunPool &P, const SliceOrder &O, int fp64_only,
+                               unsigned light_max, int leaf_size, int blocks_per_sm, unsigned long long *ctr)
+{
+    if (!fp64_only) {
+#define PB_PAIRS32(CAT)                                                                                            \
+    k_batch_pairs32<STRAT, KT, CAT><<<persistent_blocks_of(k_batch_pairs32<STRAT, KT, CAT>, blocks_per_sm), 128, 0,     \
+                                      H->stream>>>(discs, starts, slot_disc, ndisc, s0, P, O, ctr)
+        switch (cat) {
+        case CAT_GDC4: PB_PAIRS32(CAT_GDC4); break;
+        case CAT_C4: PB_PAIRS32(CAT_C4); break;
+        case CAT_S1: PB_PAIRS32(CAT_S1); break;
+        case CAT_SG1: PB_PAIRS32(CAT_SG1); break;
+        default: PB_PAIRS32(CAT_ANY); break;
         }
+#undef PB_PAIRS32
     }
-}
-
-template <int STRAT>
-static void launch_batch_kt(Handle *H, int kernel, int grid, const BatchDisc *discs, const int64_t *starts,
-                            const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m, const RunPool &P,
-                            int fp64_only, unsigned light_max, int leaf_size, unsigned long long *ctr)
-{
-#define PB_BATCH_LAUNCH(KT)                                                                                        \
-    k_batch_pairs<STRAT, KT><<<grid, 128, 0, H->stream>>>(discs, starts, slot_disc, ndisc, s0, m, P, fp64_only,     \
-                                                          light_max, leaf_size, ctr)
-    switch (kernel) {
-    case 0: PB_BATCH_LAUNCH(0); break;
-    case 1: PB_BATCH_LAUNCH(1); break;
-    case 2: PB_BATCH_LAUNCH(2); break;
-    case 3: PB_BATCH_LAUNCH(3); break;
-    case 4: PB_BATCH_LAUNCH(4); break;
-    default: PB_BATCH_LAUNCH(5); break;
-    }
-#undef PB_BATCH_LAUNCH
-}
-
-template <int STRAT>
-static int batch_blocks_per_sm()
-{
-    int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void *)k_batch_pairs<STRAT, 0>, 128, 0);
-    return per > 0 ? per : 1;
+    k_batch_pairs64<STRAT><<<persistent_blocks_of(k_batch_pairs64<STRAT>, blocks_per_sm), 128, 0, H->stream>>>(
+        discs, starts, slot_disc, ndisc, s0, m, P, O, ctr + 1);
+    k_batch_over<STRAT, KT><<<persistent_blocks_of(k_batch_over<STRAT, KT>, blocks_per_sm), 128, 0, H->stream>>>(
+        discs, starts, slot_disc, ndisc, s0, m, P, O, fp64_only, light_max, leaf_size, ctr + 2);
 }
 
 template <int STRAT>
@@ -150,45 +233,77 @@ static void launch_walk_batch(Handle *H, const BatchDisc *discs, const int64_t *
     k_batch_walk<STRAT><<<grid_for(m, 128, 1 << 30), 128, 0, H->stream>>>(discs, starts, slot_disc, ndisc, s0, m, P);
 }
 
-// one slice [s0, s0 + m) of the batch's sample points: the walk, then the sums
-cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, const BatchDisc *discs, const int64_t *starts,
+template <int STRAT>
+static void launch_slice_strat(Handle *H, int kernel, int cat, const BatchDisc *discs, const int64_t *starts,
                                const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m, const RunPool &P,
-                               int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
+                               const SliceOrder &O, int fp64_only, unsigned light_max, int leaf_size,
+                               int blocks_per_sm, unsigned long long *ctr)
+{
+#define PB_SLICE(KT)                                                                                               \
+    launch_slice_pairs<STRAT, KT>(H, cat, discs, starts, slot_disc, ndisc, s0, m, P, O, fp64_only, light_max,       \
+                                  leaf_size, blocks_per_sm, ctr)
+    switch (kernel) {
+    case 0: PB_SLICE(0); break;
+    case 1: PB_SLICE(1); break;
+    case 2: PB_SLICE(2); break;
+    case 3: PB_SLICE(3); break;
+    case 4: PB_SLICE(4); break;
+    default: PB_SLICE(5); break;
+    }
+#undef PB_SLICE
+}
+
+// One slice [s0, s0 + m) of the batch's sample points: the walk, the pair order (heaviest
+// first, overflowed last, with the FP32C/FP64 split counted on the device), then the sums.
+// ctr: [0..2] persistent-kernel counters, [3..4] pair split sums, [5] heavy count (low word).
+cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, int cat, const BatchDisc *discs,
+                               const int64_t *starts, const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m,
+                               const RunPool &P, int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
                                unsigned long long *ctr)
 {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int per;
-    switch (strategy) {   // the occupancy of the M4 instance stands for all kernels of a strategy
-    case GATHER: per = batch_blocks_per_sm<GATHER>(); break;
-    case SCATTER: per = batch_blocks_per_sm<SCATTER>(); break;
-    default: per = batch_blocks_per_sm<SYMMETRIC>(); break;
-    }
-    if (blocks_per_sm > 0 && blocks_per_sm < per) per = blocks_per_sm;
-    const int grid = sms * per;
-    cudaError_t e = cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), H->stream);
+    cudaError_t e = cudaMemsetAsync(ctr, 0, 6 * sizeof(unsigned long long), H->stream);
     if (e) return e;
     switch (strategy) {
+    case GATHER: launch_walk_batch<GATHER>(H, discs, starts, slot_disc, ndisc, s0, m, P); break;
+    case SCATTER: launch_walk_batch<SCATTER>(H, discs, starts, slot_disc, ndisc, s0, m, P); break;
+    default: launch_walk_batch<SYMMETRIC>(H, discs, starts, slot_disc, ndisc, s0, m, P); break;
+    }
+    H->launches += 1;
+    if ((e = cudaGetLastError())) return e;
+    // pair order: descending accepted count, points whose runs overflowed the pool strictly last
+    if ((e = H->lpt_k.reserve(4 * m)) || (e = H->lpt_v.reserve(4 * m)) || (e = H->lpt_ka.reserve(4 * m)) ||
+        (e = H->lpt_va.reserve(4 * m)))
+        return e;
+    k_batch_keys<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, H->lpt_k.as<uint32_t>(),
+                                                          H->lpt_v.as<uint32_t>());
+    H->launches += 1;
+    if ((e = sort_pairs_u32(H, H->lpt_k.as<uint32_t>(), H->lpt_v.as<uint32_t>(), H->lpt_ka.as<uint32_t>(),
+                            H->lpt_va.as<uint32_t>(), m, 32)))
+        return e;
+    const uint32_t *ord = H->lpt_v.as<uint32_t>();
+    unsigned *nheavy = reinterpret_cast<unsigned *>(ctr + 5);
+    if ((e = launch_count_heavy(H, P, m, fp64_only ? 0xffffffffu : light_max, nheavy, ctr + 3))) return e;
+    SliceOrder O{ord, nheavy, P.n_deferred};
+    switch (strategy) {
     case GATHER:
-        launch_walk_batch<GATHER>(H, discs, starts, slot_disc, ndisc, s0, m, P);
-        launch_batch_kt<GATHER>(H, kernel, grid, discs, starts, slot_disc, ndisc, s0, m, P, fp64_only, light_max,
-                                leaf_size, ctr);
+        launch_slice_strat<GATHER>(H, kernel, cat, discs, starts, slot_disc, ndisc, s0, m, P, O, fp64_only, light_max,
+                                   leaf_size, blocks_per_sm, ctr);
         break;
     case SCATTER:
-        launch_walk_batch<SCATTER>(H, discs, starts, slot_disc, ndisc, s0, m, P);
-        launch_batch_kt<SCATTER>(H, kernel, grid, discs, starts, slot_disc, ndisc, s0, m, P, fp64_only, light_max,
-                                 leaf_size, ctr);
+        launch_slice_strat<SCATTER>(H, kernel, cat, discs, starts, slot_disc, ndisc, s0, m, P, O, fp64_only, light_max,
+                                    leaf_size, blocks_per_sm, ctr);
         break;
     default:
-        launch_walk_batch<SYMMETRIC>(H, discs, starts, slot_disc, ndisc, s0, m, P);
-        launch_batch_kt<SYMMETRIC>(H, kernel, grid, discs, starts, slot_disc, ndisc, s0, m, P, fp64_only, light_max,
-                                   leaf_size, ctr);
+        launch_slice_strat<SYMMETRIC>(H, kernel, cat, discs, starts, slot_disc, ndisc, s0, m, P, O, fp64_only,
+                                      light_max, leaf_size, blocks_per_sm, ctr);
         break;
     }
-    H->launches += 2;
+    H->launches += 3;
     return cudaGetLastError();
 }
+
+// compile-time catalog shape of the batch's FP32C pair kernel (the host-side view of the catalog)
+int batch_catalog_shape(const DevCatalog &C32) { return catalog_shape(C32); }
 
 // the FP32-compensated payload of one disc (the single-disc launchers build it the same way)
 cudaError_t launch_batch_payload(Handle *H, const DevTree &T, const DevCatalog &C, float4 **pay, int *stride)

@@ -31,6 +31,7 @@ pb::Handle::~Handle()
     batch_desc.release();
     batch_starts.release();
     batch_slots.release();
+    batch_ctr.release();
     if (batch_host) cudaFreeHost(batch_host);
     for (auto &b : in_cols) b.release();
     for (auto &b : cols_s) b.release();
@@ -1501,7 +1502,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
     CK(H.batch_desc.reserve(desc_bytes));
     CK(H.batch_starts.reserve(start_bytes));
     CK(H.batch_slots.reserve(slot_bytes));
-    CK(H.counter.reserve(sizeof(unsigned long long)));
+    CK(H.batch_ctr.reserve(6 * sizeof(unsigned long long)));
     BatchDisc *hd = static_cast<BatchDisc *>(H.batch_host);
     int64_t *hs = reinterpret_cast<int64_t *>(static_cast<char *>(H.batch_host) + desc_bytes);
     uint32_t *ho = reinterpret_cast<uint32_t *>(static_cast<char *>(H.batch_host) + desc_bytes + start_bytes);
@@ -1532,6 +1533,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
         }
         hd[k] = D;
     }
+    const int cat_shape = batch_catalog_shape(hd[0].C32);
     CK(cudaMemcpyAsync(H.batch_desc.p, H.batch_host, desc_bytes, cudaMemcpyHostToDevice, H.stream));
     CK(cudaMemcpyAsync(H.batch_starts.p, hs, start_bytes, cudaMemcpyHostToDevice, H.stream));
     CK(cudaMemcpyAsync(H.batch_slots.p, ho, slot_bytes, cudaMemcpyHostToDevice, H.stream));
@@ -1570,10 +1572,10 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
             CK(cudaMemsetAsync(ctr, 0, 16, H.stream));
             CK(cudaMemsetAsync(P.qacc, 0, sizeof(unsigned) * m, H.stream));
             CK(cudaMemsetAsync(P.qflag, 0, sizeof(int) * m, H.stream));
-            CK(launch_batch_slice(&H, strategy, H.kernel, H.batch_desc.as<BatchDisc>(), H.batch_starts.as<int64_t>(),
-                                  H.batch_slots.as<uint32_t>(), ndiscs, s0, m, P, precision == PB_FP64 ? 1 : 0,
-                                  (unsigned)H.light_max, H.leaf_size, H.batch_blocks,
-                                  H.counter.as<unsigned long long>()));
+            CK(launch_batch_slice(&H, strategy, H.kernel, cat_shape, H.batch_desc.as<BatchDisc>(),
+                                  H.batch_starts.as<int64_t>(), H.batch_slots.as<uint32_t>(), ndiscs, s0, m, P,
+                                  precision == PB_FP64 ? 1 : 0, (unsigned)H.light_max, H.leaf_size, H.batch_blocks,
+                                  H.batch_ctr.as<unsigned long long>()));
         }
     }
     if (flags & PB_BATCH_ASYNC) return PB_OK;

@@ -102,17 +102,17 @@ __device__ __forceinline__ const float4 *rec_of(const float4 *pay, int stride, u
 // the DevCatalog at run time; 1: four columns, gradient + divergence + curl; 2: four columns,
 // curl only; 3: one column, scalars only.  A specialised kernel performs exactly the
 // operations, in the same order, that the generic one performs for such a catalog.
-constexpr int CAT_ANY = 0, CAT_GDC4 = 1, CAT_C4 = 2, CAT_S1 = 3;
+constexpr int CAT_ANY = 0, CAT_GDC4 = 1, CAT_C4 = 2, CAT_S1 = 3, CAT_SG1 = 4;   // SG1: one column, scalar + gradient
 
 template <int CAT>
 struct CatShape {
     __device__ static __forceinline__ int nu(const DevCatalog &C)
     {
-        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 4 : (CAT == CAT_S1 ? 1 : C.nU);
+        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 4 : ((CAT == CAT_S1 || CAT == CAT_SG1) ? 1 : C.nU);
     }
     __device__ static __forceinline__ bool grad(const DevCatalog &C)
     {
-        return CAT == CAT_GDC4 ? true : (CAT == CAT_ANY ? C.n_grad > 0 : false);
+        return (CAT == CAT_GDC4 || CAT == CAT_SG1) ? true : (CAT == CAT_ANY ? C.n_grad > 0 : false);
     }
     __device__ static __forceinline__ bool div(const DevCatalog &C)
     {
@@ -125,7 +125,7 @@ struct CatShape {
     __device__ static __forceinline__ bool any(const DevCatalog &C) { return grad(C) || div(C) || curl(C); }
     __device__ static __forceinline__ int stride(int s)
     {
-        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 5 : (CAT == CAT_S1 ? 3 : s);
+        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 5 : ((CAT == CAT_S1 || CAT == CAT_SG1) ? 3 : s);
     }
 };
 
@@ -134,6 +134,7 @@ inline int catalog_shape(const DevCatalog &C)
     if (C.nU == 4 && C.n_grad == 1 && C.g_u[0] == 0 && C.n_div == 1 && C.n_curl == 1) return CAT_GDC4;
     if (C.nU == 4 && C.n_grad == 0 && C.n_div == 0 && C.n_curl == 1) return CAT_C4;
     if (C.nU == 1 && C.n_grad == 0 && C.n_div == 0 && C.n_curl == 0) return CAT_S1;
+    if (C.nU == 1 && C.n_grad == 1 && C.g_u[0] == 0 && C.n_div == 0 && C.n_curl == 0) return CAT_SG1;
     return CAT_ANY;
 }
 

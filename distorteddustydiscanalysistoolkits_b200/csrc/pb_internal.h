@@ -106,7 +106,7 @@ struct Handle {
     int64_t split_hq = 0, split_lq = 0, split_hp = 0, split_lp = 0;
 
     // batched launch (pb_batch_points): descriptors, processing-order starts, pinned staging
-    DBuf batch_desc, batch_starts, batch_slots;
+    DBuf batch_desc, batch_starts, batch_slots, batch_ctr;
     void *batch_host = nullptr;
     size_t batch_host_bytes = 0;
     int leaf_size = 1;       // warp-uniform walk: subtrees of at most this many leaves are scanned
@@ -159,6 +159,9 @@ cudaError_t launch_lpt_order(Handle *H, const RunPool &P, int64_t m, uint32_t **
 cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned light_max, bool plain,
                                uint32_t **order, int64_t *m_heavy, unsigned long long *pairs);
 cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out);
+cudaError_t launch_count_heavy(Handle *H, const RunPool &P, int64_t m, unsigned light_max, unsigned *count,
+                               unsigned long long *pairs);
+int batch_catalog_shape(const DevCatalog &C32);
 
 // ---- launchers (pb_sched.cu) ----
 cudaError_t launch_sched_features(Handle *H, const DevTree &T, int64_t m, const uint32_t *ql, const double *qx,
@@ -205,9 +208,9 @@ cudaError_t launch_stats(Handle *H, const DevTree &T, int strategy, int64_t nq, 
 struct LineFrame {
     double c[3], e1[3], e2[3], d[3];
 };
-cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, const BatchDisc *discs, const int64_t *starts,
-                               const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m, const RunPool &P,
-                               int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
+cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, int cat, const BatchDisc *discs,
+                               const int64_t *starts, const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m,
+                               const RunPool &P, int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
                                unsigned long long *ctr);
 cudaError_t launch_batch_payload(Handle *H, const DevTree &T, const DevCatalog &C, float4 **pay, int *stride);
 cudaError_t launch_line_image(Handle *H, const double *a0, int64_t n0, const double *a1, int64_t n1, const LineFrame &F,

@@ -148,6 +148,7 @@ static void launch_pairs_cat(Handle *H, const DevTree &T, const DevCatalog &C, c
     case CAT_GDC4: launch_pairs_one<STRAT, KT, CAT_GDC4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     case CAT_C4: launch_pairs_one<STRAT, KT, CAT_C4>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     case CAT_S1: launch_pairs_one<STRAT, KT, CAT_S1>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
+    case CAT_SG1: launch_pairs_one<STRAT, KT, CAT_SG1>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     default: launch_pairs_one<STRAT, KT, CAT_ANY>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     }
 }

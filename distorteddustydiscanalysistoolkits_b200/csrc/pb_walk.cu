@@ -392,6 +392,18 @@ cudaError_t launch_split_order(Handle *H, const RunPool &P, int64_t m, unsigned 
     return cudaSuccess;
 }
 
+// the FP32C/FP64 split of a walked slice, left on the device: *count (zeroed here) = queries
+// with more than light_max accepted leaves, pairs[0..1] += their pairs / the other queries' pairs
+cudaError_t launch_count_heavy(Handle *H, const RunPool &P, int64_t m, unsigned light_max, unsigned *count,
+                               unsigned long long *pairs)
+{
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned), H->stream);
+    if (e) return e;
+    k_count_heavy<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, light_max, count, pairs);
+    H->launches += 1;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_iota(Handle *H, int64_t m, uint32_t *out)
 {
     k_iota<<<grid_for(m, 256), 256, 0, H->stream>>>(m, out);
