@@ -48,6 +48,9 @@ sys.path.insert(0, REPO)
 METRIC = "interp grid pts/s (LBVH build ms reported beside it)"
 UNIT = "grid pts/s"
 L2_FLUSH_BYTES = 256 << 20
+# thread instructions per pair of k_pairs32w<itpSymmetric, M4, grad+div+curl> measured by ncu
+# (smsp__inst_executed.sum x 32 / pairs; profiles/k_pairs32w_c2disc_96x96x24.md)
+PAIRS32_THREAD_INST_PER_PAIR = 149.4
 
 
 def parse():
@@ -649,11 +652,26 @@ def main():
                 args.particles in (None, 1 << 21) and args.grid in (None, "256,256,64"):
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")
         achieved = per[dom]["achieved_gbs"]
+        # The pair kernel is bound by instruction issue, not by DRAM (its DRAM traffic is 3 % of
+        # peak; the records are re-read from L2): pairs/s against the issue ceiling, SMs x 4
+        # schedulers x SM clock / warp instructions per pair, with the instructions per pair of
+        # the committed ncu capture of k_pairs32w (profiles/k_pairs32w_c2disc_96x96x24.md)
+        issue = None
+        acc_pairs = float(stats[:, 4].astype(np.float64).sum())
+        if prec == pb.FP32C and ph[2] > 0:
+            props = torch.cuda.get_device_properties(local)
+            sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+            warp_inst_per_pair = PAIRS32_THREAD_INST_PER_PAIR / 32.0
+            ceiling = props.multi_processor_count * 4 * sm_mhz * 1e6 / warp_inst_per_pair
+            got = acc_pairs / (ph[2] / 1e3)
+            issue = {"pairs_per_s": got, "issue_ceiling_pairs_per_s": ceiling, "frac": got / ceiling,
+                     "thread_inst_per_pair": PAIRS32_THREAD_INST_PER_PAIR, "sm_mhz": sm_mhz,
+                     "note": "issue ceiling = SMs x 4 schedulers x SM clock / (thread instructions per pair / 32)"}
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None, "traffic": traffic,
                     "kernel": per[dom]["kernel"], "algorithmic_bytes_per_launch": alg[dom],
                     "peak_source": peak_source,
-                    "phases": per,
+                    "phases": per, "pair_issue": issue,
                     "events_per_query": {k: float(stats[:, i].mean()) for i, k in enumerate(
                         ("nearest_internal", "nearest_leaf", "main_internal", "main_leaf", "accepted"))}}
 
