@@ -1,6 +1,7 @@
 """Error statistics of interpolated fields against a reference evaluation of the same fields.
 
-Two measures per field, both over the points where the reference value is not NaN:
+Two measures per field, both over the points where neither value is NaN (a NaN in one field
+and not in the other is counted as a ``nan_mismatch``):
   field-scaled   |got - ref| / max|ref|  (the error relative to the field's magnitude);
   pointwise      |got - ref| / |ref| over the points with |ref| >= floor * max|ref|
                  (the relative error of each value; the floor leaves out the neighbourhood of
@@ -21,7 +22,7 @@ def field_errors(got, ref, names=None, floor=POINTWISE_FLOOR):
     for name, a, r in zip(names, got, ref):
         a = np.asarray(a, np.float64)
         r = np.asarray(r, np.float64)
-        ok = ~np.isnan(r)
+        ok = ~np.isnan(r) & ~np.isnan(a)
         e = {"nan_mismatch": int(np.count_nonzero(np.isnan(a) != np.isnan(r))), "points": int(ok.sum())}
         if ok.any():
             sc = float(np.max(np.abs(r[ok])))
@@ -42,5 +43,7 @@ def field_errors(got, ref, names=None, floor=POINTWISE_FLOOR):
 
 
 def worst(stats, key):
-    """Largest value of ``key`` over the fields of a field_errors result (0 if absent)."""
-    return max((v.get(key, 0.0) for v in stats.values()), default=0.0)
+    """Largest value of ``key`` over the fields of a field_errors result (0 if absent; a NaN
+    value counts as infinite, so it is never hidden by the order of the fields)."""
+    vals = [v.get(key, 0.0) for v in stats.values()]
+    return max((float("inf") if v != v else v for v in vals), default=0.0)
