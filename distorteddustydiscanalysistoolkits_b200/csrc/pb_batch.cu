@@ -73,13 +73,22 @@ __global__ void __launch_bounds__(128) k_batch_walk(const BatchDisc *__restrict_
     }
 }
 
-// sort keys of a slice's pair order: 0x7fffffff - accepted (heaviest first); overflowed last
+// Sort keys of a slice's pair order: class (FP32C points, then FP64 points, then points whose
+// runs overflowed the pool), then the disc's processing slot, then descending accepted count
+// (clipped to the count bits left after the slot's).  Grouping a class by disc keeps the
+// points that run at the same time on one disc's tree and payload, so the L2 holds one disc's
+// working set instead of all of them; heaviest first inside a disc keeps the tail short.
 __global__ void k_batch_keys(int64_t m, const unsigned *__restrict__ qacc, const int *__restrict__ qflag,
-                             uint32_t *keys, uint32_t *vals)
+                             const int64_t *__restrict__ starts, int ndisc, int64_t s0, unsigned light_max,
+                             int slot_bits, uint32_t *keys, uint32_t *vals)
 {
+    const int cbits = 30 - slot_bits;
+    const unsigned cmask = cbits >= 32 ? 0xffffffffu : ((1u << cbits) - 1u);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
         const unsigned a = qacc[t];
-        keys[t] = qflag[t] ? 0x80000000u : 0x7fffffffu - (a > 0x7fffffffu ? 0x7fffffffu : a);
+        const unsigned cls = qflag[t] ? 2u : (a > light_max ? 0u : 1u);
+        const unsigned slot = (unsigned)batch_slot(starts, ndisc, s0 + t);
+        keys[t] = (cls << 30) | (slot << cbits) | (cmask - (a > cmask ? cmask : a));
         vals[t] = (uint32_t)t;
     }
 }
@@ -101,7 +110,7 @@ struct DescCache {
     }
 };
 
-// the slice's points in pair order (heaviest first, overflowed last): positions [0, nheavy)
+// the slice's points in pair order (k_batch_keys): positions [0, nheavy)
 // are FP32C points, [nheavy, m - nover) FP64 points, [m - nover, m) points whose runs did not
 // fit the pool; ord[t] is the slice-local point
 struct SliceOrder {
@@ -270,12 +279,15 @@ cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, int cat, con
     }
     H->launches += 1;
     if ((e = cudaGetLastError())) return e;
-    // pair order: descending accepted count, points whose runs overflowed the pool strictly last
+    // pair order: FP32C points, FP64 points, overflowed points; by disc inside a class
     if ((e = H->lpt_k.reserve(4 * m)) || (e = H->lpt_v.reserve(4 * m)) || (e = H->lpt_ka.reserve(4 * m)) ||
         (e = H->lpt_va.reserve(4 * m)))
         return e;
-    k_batch_keys<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, H->lpt_k.as<uint32_t>(),
-                                                          H->lpt_v.as<uint32_t>());
+    int slot_bits = 0;
+    while ((1 << slot_bits) < ndisc && slot_bits < 30) ++slot_bits;
+    k_batch_keys<<<grid_for(m, 256), 256, 0, H->stream>>>(m, P.qacc, P.qflag, starts, ndisc, s0,
+                                                          fp64_only ? 0xffffffffu : light_max, slot_bits,
+                                                          H->lpt_k.as<uint32_t>(), H->lpt_v.as<uint32_t>());
     H->launches += 1;
     if ((e = sort_pairs_u32(H, H->lpt_k.as<uint32_t>(), H->lpt_v.as<uint32_t>(), H->lpt_ka.as<uint32_t>(),
                             H->lpt_va.as<uint32_t>(), m, 32)))

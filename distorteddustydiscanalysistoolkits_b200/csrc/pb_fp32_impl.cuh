@@ -8,7 +8,7 @@
 
 namespace pb {
 
-constexpr int CHUNK = 16;
+constexpr int CHUNK = 32;
 static_assert(CHUNK % 4 == 0, "groups of two or four batches must not straddle a flush");
 
 // ---- kernel shapes f(q), f'(q) for q >= 0 (kernels/*.jl) in FP32 ----
@@ -258,13 +258,13 @@ struct Terms32 {
     float w, a[MAXU], gx, gy, gz;
 };
 
+// the terms of the pair with the particle whose record (field 0) is `rec`
 template <int STRAT, int KT, int CAT>
 __device__ __forceinline__ void terms32(const Acc32 &A, const DevCatalog &C, const Query32 &Q,
-                                        const float4 *__restrict__ pay, int stride, int b, Terms32 &t)
+                                        const float4 *__restrict__ rec, int stride, Terms32 &t)
 {
     stride = CatShape<CAT>::stride(stride);
     const bool need_grad = CatShape<CAT>::any(C);
-    const float4 *rec = rec_of(pay, stride, b);
     const float4 p0 = __ldg(rec), p1 = __ldg(rec + PAY_BLOCK);
     const float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
     const float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
@@ -272,22 +272,23 @@ __device__ __forceinline__ void terms32(const Acc32 &A, const DevCatalog &C, con
     float cWb, cGb, ch[MAXU], cl[MAXU];
     load_cols<CAT>(rec, stride, cWb, cGb, ch, cl);
     const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+    // the SFU's reciprocal square root without the subnormal-input path of rsqrtf (the
+    // approximation is the same for normal inputs); a pair closer than 1e-15 (r2 <= 1e-30)
+    // counts as coincident, as r2 = 0 does: no gradient term, W at q = 0
+    float rs;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rs) : "f"(r2));
+    const float rinv = r2 > 1e-30f ? rs : 0.f;
     const float r = r2 * rinv;
     float W, G;
     if (STRAT == SYMMETRIC) {
         float fa, dfa;
         shape<KT>(r * Q.ih, fa, dfa);
-        // W(r, h_b) and its derivative are exactly zero outside the neighbour's own support;
-        // when that holds on every lane the h_b term is skipped (it would add exact zeros)
-        const float qb = r * p0.w;
-        float Wb = 0.f, Gb = 0.f;
-        if (__any_sync(__activemask(), qb < ksupport(KT))) {
-            float fb, dfb;
-            shape<KT>(qb, fb, dfb);
-            Wb = cWb * fb;
-            Gb = cGb * dfb;
-        }
+        // W(r, h_b) and its derivative: every piece of a shape clamps to zero outside the
+        // neighbour's own support, so there the h_b term adds zeros; it is evaluated on every
+        // lane (a warp vote to skip it costs more issue slots than it saves)
+        float fb, dfb;
+        shape<KT>(r * p0.w, fb, dfb);
+        const float Wb = cWb * fb, Gb = cGb * dfb;
         W = 0.5f * fmaf(Q.cw, fa, Wb);
         G = (0.5f * fmaf(Q.cg, dfa, Gb)) * rinv;
     } else if (STRAT == GATHER) {
@@ -343,19 +344,21 @@ __device__ __forceinline__ void pair32(Acc32 &A, const DevCatalog &C, const Quer
                                        const float4 *__restrict__ pay, int stride, int b)
 {
     Terms32 t;
-    terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b, t);
+    terms32<STRAT, KT, CAT>(A, C, Q, rec_of(pay, CatShape<CAT>::stride(stride), b), stride, t);
     accum32<CAT>(A, C, t);
 }
 
-// two pairs of one lane (consecutive in its sequence): independent terms, then accumulated
-// in order -- the same arithmetic as two pair32 calls, with twice the independent work
+// two pairs of one lane, with particles b and b + 32 (the same lane of two consecutive full
+// batches inside one run; r1 is b's record, so b + 32's is one payload block further):
+// independent terms, then accumulated in order -- the same arithmetic as two pair32 calls,
+// with twice the independent work
 template <int STRAT, int KT, int CAT>
 __device__ __forceinline__ void pair32x2(Acc32 &A, const DevCatalog &C, const Query32 &Q,
-                                         const float4 *__restrict__ pay, int stride, int b1, int b2)
+                                         const float4 *__restrict__ r1, int stride)
 {
     Terms32 t1, t2;
-    terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b1, t1);
-    terms32<STRAT, KT, CAT>(A, C, Q, pay, stride, b2, t2);
+    terms32<STRAT, KT, CAT>(A, C, Q, r1, stride, t1);
+    terms32<STRAT, KT, CAT>(A, C, Q, r1 + CatShape<CAT>::stride(stride) * PAY_BLOCK, stride, t2);
     accum32<CAT>(A, C, t1);
     accum32<CAT>(A, C, t2);
 }
@@ -523,8 +526,9 @@ __device__ __forceinline__ void pairs32_query(const DevTree &T, const DevCatalog
             nb = 0;
         }
     };
+    const int S = CatShape<CAT>::stride(stride);
     auto two = [&](int m1) {   // flush boundary after the second batch (nb is even here)
-        pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
+        pair32x2<STRAT, KT, CAT>(A, C, Q, rec_of(pay, S, m1), stride);
         nb += 2;
         if (nb == CHUNK) {
             A.flush<CAT>(C);
@@ -532,8 +536,9 @@ __device__ __forceinline__ void pairs32_query(const DevTree &T, const DevCatalog
         }
     };
     auto four = [&](int m1) {   // flush boundary after the fourth batch (nb is a multiple of 4 here)
-        pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1, m1 + 32);
-        pair32x2<STRAT, KT, CAT>(A, C, Q, pay, stride, m1 + 64, m1 + 96);
+        const float4 *r1 = rec_of(pay, S, m1);   // m1 + 64 is two payload blocks further
+        pair32x2<STRAT, KT, CAT>(A, C, Q, r1, stride);
+        pair32x2<STRAT, KT, CAT>(A, C, Q, r1 + 2 * S * PAY_BLOCK, stride);
         nb += 4;
         if (nb == CHUNK) {
             A.flush<CAT>(C);
