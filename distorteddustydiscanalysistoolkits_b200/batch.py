@@ -173,9 +173,10 @@ class DeviceBatch:
     def npoints(self):
         return int(sum(self.npts))
 
-    def set_options(self, leaf_size=1, order=0, blocks_per_sm=0):
+    def set_options(self, leaf_size=1, order=0, blocks_per_sm=0, walk_split=16):
         H = self.backends[0].handle
         H.set_option("leaf_size", int(leaf_size))
+        H.set_option("batch_walk_split", int(walk_split))
         H.set_option("batch_order", int(order))
         H.set_option("batch_blocks_per_sm", int(blocks_per_sm))
 
@@ -237,16 +238,17 @@ class BatchAutotuner:
     """Schedule options of a DeviceBatch (outputs do not depend on them): every combination of
     the candidates is captured and timed over `repeats` graph replays; the fastest is kept."""
 
-    def __init__(self, leaf_size=(1, 4, 8, 16), order=(0, 1), blocks_per_sm=(0, 2), repeats=2):
-        self.grid = {"leaf_size": leaf_size, "order": order, "blocks_per_sm": blocks_per_sm}
+    def __init__(self, leaf_size=(1, 4, 8, 16), order=(0, 1), blocks_per_sm=(0, 2), walk_split=(8, 16, 32),
+                 repeats=2):
+        self.grid = {"leaf_size": leaf_size, "order": order, "blocks_per_sm": blocks_per_sm, "walk_split": walk_split}
         self.repeats = repeats
         self.best = None
         self.timings = []
 
     def tune(self, batch):
         best, best_ms = None, math.inf
-        for ls, od, bp in itertools.product(*self.grid.values()):
-            opts = {"leaf_size": ls, "order": od, "blocks_per_sm": bp}
+        for ls, od, bp, ws in itertools.product(*self.grid.values()):
+            opts = {"leaf_size": ls, "order": od, "blocks_per_sm": bp, "walk_split": ws}
             batch.set_options(**opts)
             batch.capture()
             ms = batch.timed(self.repeats)

@@ -1,10 +1,12 @@
 // pb_batch.cu -- the point interpolation of many snapshots (discs) at once, each disc with its
 // own LBVH, particles, grid and outputs.  The sample points of all discs form one index space
 // (disc after disc, in the processing order the host chose), cut into slices of a fixed size.
-// Per slice, two persistent launches cover every disc:
-//   1. k_batch_walk: one thread per sample point finds its disc (binary search over the discs'
-//      first indices), its nearest particle, and walks the disc's tree, appending the accepted
-//      leaves as runs to a shared pool (the walk of the single-disc path, whole tree per point);
+// Per slice, these launches cover every disc:
+//   1. k_batch_nearest + k_batch_walk_items: one thread per sample point finds its disc (binary
+//      search over the discs' first indices) and its nearest particle; then warps walk
+//      (32 points, subtree) items -- every disc's tree is cut into subtrees on the device
+//      after its build -- appending the accepted leaves as runs to a shared pool (the
+//      single-disc path's item walk);
 //   2. k_batch_pairs: one warp per sample point sums its runs with the bodies of the single-disc
 //      pair kernels -- FP64 (the reference's arithmetic) for FP64 mode and for FP32C points of at
 //      most light_max accepted neighbours, FP32-compensated for heavier ones -- and a point whose
@@ -54,22 +56,61 @@ __device__ __forceinline__ int batch_slot(const int64_t *__restrict__ starts, in
     return lo;
 }
 
+// per point of the slice: its disc's processing slot and, for gather/symmetric, its nearest
+// particle (LBVH_find_nearest_h)
 template <int STRAT>
-__global__ void __launch_bounds__(128) k_batch_walk(const BatchDisc *__restrict__ discs,
-                                                    const int64_t *__restrict__ starts,
-                                                    const uint32_t *__restrict__ slot_disc, int ndisc, int64_t s0,
-                                                    int64_t m, RunPool P)
+__global__ void __launch_bounds__(128) k_batch_nearest(const BatchDisc *__restrict__ discs,
+                                                       const int64_t *__restrict__ starts,
+                                                       const uint32_t *__restrict__ slot_disc, int ndisc, int64_t s0,
+                                                       int64_t m, RunPool P, int *slot_of)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t j = s0 + t;
         const int lo = batch_slot(starts, ndisc, j);
-        const BatchDisc &D = discs[__ldg(slot_disc + lo)];
-        const DevTree T = D.T;
-        const int64_t qi = j - __ldg(starts + lo);
-        const double px = __ldg(D.qx + qi), py = __ldg(D.qy + qi), pz = __ldg(D.qz + qi);
-        const int64_t bnear = STRAT != SCATTER ? nearest_leaf(T, px, py, pz) : -1;
+        slot_of[t] = lo;
+        int64_t bnear = -1;
+        if (STRAT != SCATTER) {
+            const BatchDisc &D = discs[__ldg(slot_disc + lo)];
+            const int64_t qi = j - __ldg(starts + lo);
+            bnear = nearest_leaf(D.T, __ldg(D.qx + qi), __ldg(D.qy + qi), __ldg(D.qz + qi));
+        }
         P.bnear[t] = (int)bnear;
-        walk_item_at<STRAT>(T, P, t, 0, (uint32_t)t, px, py, pz, kernel_valid(T.kernel));
+    }
+}
+
+// The walk of a slice as warp items (32 consecutive points, subtree s), point blocks
+// outermost: lane l walks subtree s of the cut of its own point's disc (the lanes of a warp
+// share a disc except where the block straddles two) and writes the (point, subtree) item;
+// an s past the disc's cut gets an empty item.  The items of a point, read in subtree order,
+// list its accepted leaves in the reference's DFS order, as the whole-tree walk does.
+template <int STRAT>
+__global__ void __launch_bounds__(128) k_batch_walk_items(const BatchDisc *__restrict__ discs,
+                                                          const int64_t *__restrict__ starts,
+                                                          const uint32_t *__restrict__ slot_disc,
+                                                          const int *__restrict__ slot_of, int64_t s0, int64_t m,
+                                                          RunPool P, unsigned long long *counter)
+{
+    const int lane = threadIdx.x & 31;
+    const int ns = P.ns;
+    const int64_t nitems = ((m + 31) / 32) * ns;
+    for (;;) {
+        unsigned long long wi = 0;
+        if (lane == 0) wi = atomicAdd(counter, 1ULL);
+        wi = __shfl_sync(0xffffffffu, wi, 0);
+        if ((int64_t)wi >= nitems) break;
+        const int64_t t = (int64_t)(wi / ns) * 32 + lane;
+        const int s = (int)(wi % ns);
+        if (t >= m) continue;
+        const int lo = __ldg(slot_of + t);
+        const BatchDisc &D = discs[__ldg(slot_disc + lo)];
+        if (s >= __ldg(D.ncut)) {
+            P.items[t * ns + s] = make_int2(-1, 0);
+            continue;
+        }
+        const DevTree T = D.T;
+        const int64_t qi = s0 + t - __ldg(starts + lo);
+        walk_item_at<STRAT>(T, P, D.cut, t, s, (uint32_t)t, __ldg(D.qx + qi), __ldg(D.qy + qi), __ldg(D.qz + qi),
+                            kernel_valid(T.kernel));
     }
 }
 
@@ -237,9 +278,13 @@ static void launch_slice_pairs(Handle *H, int cat, const BatchDisc *discs, const
 
 template <int STRAT>
 static void launch_walk_batch(Handle *H, const BatchDisc *discs, const int64_t *starts, const uint32_t *slot_disc,
-                              int ndisc, int64_t s0, int64_t m, const RunPool &P)
+                              int ndisc, int64_t s0, int64_t m, const RunPool &P, int *slot_of,
+                              unsigned long long *counter)
 {
-    k_batch_walk<STRAT><<<grid_for(m, 128, 1 << 30), 128, 0, H->stream>>>(discs, starts, slot_disc, ndisc, s0, m, P);
+    k_batch_nearest<STRAT><<<grid_for(m, 128, 1 << 30), 128, 0, H->stream>>>(discs, starts, slot_disc, ndisc, s0, m, P,
+                                                                          slot_of);
+    k_batch_walk_items<STRAT><<<persistent_blocks_of(k_batch_walk_items<STRAT>, 0), 128, 0, H->stream>>>(
+        discs, starts, slot_disc, slot_of, s0, m, P, counter);
 }
 
 template <int STRAT>
@@ -262,22 +307,24 @@ static void launch_slice_strat(Handle *H, int kernel, int cat, const BatchDisc *
 #undef PB_SLICE
 }
 
-// One slice [s0, s0 + m) of the batch's sample points: the walk, the pair order (heaviest
-// first, overflowed last, with the FP32C/FP64 split counted on the device), then the sums.
-// ctr: [0..2] persistent-kernel counters, [3..4] pair split sums, [5] heavy count (low word).
+// One slice [s0, s0 + m) of the batch's sample points: nearest particles, the walk over
+// (point, subtree) items, the pair order (by class, then disc, with the FP32C/FP64 split
+// counted on the device), then the sums.  slot_of holds m ints.
+// ctr: [0..2] persistent pair-kernel counters, [3..4] pair split sums, [5] heavy count (low
+// word), [6] walk queue.
 cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, int cat, const BatchDisc *discs,
                                const int64_t *starts, const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m,
                                const RunPool &P, int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
-                               unsigned long long *ctr)
+                               int *slot_of, unsigned long long *ctr)
 {
-    cudaError_t e = cudaMemsetAsync(ctr, 0, 6 * sizeof(unsigned long long), H->stream);
+    cudaError_t e = cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), H->stream);
     if (e) return e;
     switch (strategy) {
-    case GATHER: launch_walk_batch<GATHER>(H, discs, starts, slot_disc, ndisc, s0, m, P); break;
-    case SCATTER: launch_walk_batch<SCATTER>(H, discs, starts, slot_disc, ndisc, s0, m, P); break;
-    default: launch_walk_batch<SYMMETRIC>(H, discs, starts, slot_disc, ndisc, s0, m, P); break;
+    case GATHER: launch_walk_batch<GATHER>(H, discs, starts, slot_disc, ndisc, s0, m, P, slot_of, ctr + 6); break;
+    case SCATTER: launch_walk_batch<SCATTER>(H, discs, starts, slot_disc, ndisc, s0, m, P, slot_of, ctr + 6); break;
+    default: launch_walk_batch<SYMMETRIC>(H, discs, starts, slot_disc, ndisc, s0, m, P, slot_of, ctr + 6); break;
     }
-    H->launches += 1;
+    H->launches += 2;
     if ((e = cudaGetLastError())) return e;
     // pair order: FP32C points, FP64 points, overflowed points; by disc inside a class
     if ((e = H->lpt_k.reserve(4 * m)) || (e = H->lpt_v.reserve(4 * m)) || (e = H->lpt_ka.reserve(4 * m)) ||

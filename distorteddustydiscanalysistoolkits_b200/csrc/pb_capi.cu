@@ -946,6 +946,9 @@ int32_t pb_set_option(pb_handle *h, const char *name, int64_t value)
     } else if (!strcmp(name, "batch_blocks_per_sm")) {
         if (value < 0 || value > 32) return fail(H, PB_ERR_INVALID, "batch_blocks_per_sm must be in 0..32");
         H.batch_blocks = (int)value;
+    } else if (!strcmp(name, "batch_walk_split")) {
+        if (value < 1 || value > 1024) return fail(H, PB_ERR_INVALID, "batch_walk_split must be in 1..1024");
+        H.batch_walk_split = (int)value;
     } else if (!strcmp(name, "walk_split")) {
         if (value < 1 || value > 4096) return fail(H, PB_ERR_INVALID, "walk_split must be in 1..4096");
         H.walk_split = (int)value;
@@ -1491,7 +1494,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
     // pinned staging: descriptors, starts (processing order) and slot -> disc
     const size_t desc_bytes = sizeof(BatchDisc) * ndiscs, start_bytes = sizeof(int64_t) * (ndiscs + 1),
                  slot_bytes = sizeof(uint32_t) * ndiscs;
-    const size_t host_bytes = desc_bytes + start_bytes + slot_bytes + sizeof(int2);
+    const size_t host_bytes = desc_bytes + start_bytes + slot_bytes;
     if (H.batch_host_bytes < host_bytes) {
         if (H.batch_host) cudaFreeHost(H.batch_host);
         H.batch_host = nullptr;
@@ -1502,7 +1505,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
     CK(H.batch_desc.reserve(desc_bytes));
     CK(H.batch_starts.reserve(start_bytes));
     CK(H.batch_slots.reserve(slot_bytes));
-    CK(H.batch_ctr.reserve(6 * sizeof(unsigned long long)));
+    CK(H.batch_ctr.reserve(8 * sizeof(unsigned long long)));
     BatchDisc *hd = static_cast<BatchDisc *>(H.batch_host);
     int64_t *hs = reinterpret_cast<int64_t *>(static_cast<char *>(H.batch_host) + desc_bytes);
     uint32_t *ho = reinterpret_cast<uint32_t *>(static_cast<char *>(H.batch_host) + desc_bytes + start_bytes);
@@ -1524,6 +1527,8 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
         D.qy = qy[k];
         D.qz = qz[k];
         D.nq = npts[k];
+        // the disc's walk cut, made on the device from the tree just built
+        CK(launch_cut_device(&Hk, D.T, H.batch_walk_split, &D.cut, &D.ncut));
         if (precision == PB_FP32C) {
             float4 *pay = nullptr;
             int stride = 0;
@@ -1539,26 +1544,25 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
     CK(cudaMemcpyAsync(H.batch_slots.p, ho, slot_bytes, cudaMemcpyHostToDevice, H.stream));
     // slices of a fixed size share one run pool, sized once (a call that reuses it allocates
     // nothing, which is what lets a step be captured in a CUDA graph)
+    // (point, subtree) item records per point: the largest cut launch_cut_device can make
+    const int NS = 4 * H.batch_walk_split + 8;
     const int64_t S = std::max<int64_t>(1, std::min<int64_t>(H.slice > 0 ? H.slice : qtotal, qtotal));
-    if (qtotal > 0 && (H.pool_cap == 0 || H.batch_slice < S)) {
-        int rc = reserve_pool(H, S, 1);
+    if (qtotal > 0 && (H.pool_cap == 0 || H.batch_slice < S || H.batch_ns < NS)) {
+        int rc = reserve_pool(H, S, NS);
         if (rc) return rc;
         H.batch_slice = S;
+        H.batch_ns = NS;
     }
     if (qtotal > 0) {
-        // the cut of a batch: every tree whole (root 1, stop 0), staged in pinned memory
-        int2 *hcut = reinterpret_cast<int2 *>(static_cast<char *>(H.batch_host) + desc_bytes + start_bytes + slot_bytes);
-        *hcut = make_int2(1, 0);
-        CK(H.cut.reserve(sizeof(int2)));
-        CK(cudaMemcpyAsync(H.cut.p, hcut, sizeof(int2), cudaMemcpyHostToDevice, H.stream));
+        CK(H.batch_slot_of.reserve(sizeof(int) * H.batch_slice));
         unsigned long long *ctr = H.pool_ctr.as<unsigned long long>();
         RunPool P;
         P.runs = H.pool_runs.as<uint2>();
         P.next = H.pool_next.as<int>();
         P.used = ctr;
         P.cap = H.pool_cap;
-        P.ns = 1;
-        P.cut = H.cut.as<int2>();
+        P.ns = NS;
+        P.cut = nullptr;   // every disc's own cut is in its descriptor
         P.items = H.items.as<int2>();
         P.bnear = H.wbnear.as<int>();
         P.qacc = H.qacc.as<unsigned>();
@@ -1575,7 +1579,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
             CK(launch_batch_slice(&H, strategy, H.kernel, cat_shape, H.batch_desc.as<BatchDisc>(),
                                   H.batch_starts.as<int64_t>(), H.batch_slots.as<uint32_t>(), ndiscs, s0, m, P,
                                   precision == PB_FP64 ? 1 : 0, (unsigned)H.light_max, H.leaf_size, H.batch_blocks,
-                                  H.batch_ctr.as<unsigned long long>()));
+                                  H.batch_slot_of.as<int>(), H.batch_ctr.as<unsigned long long>()));
         }
     }
     if (flags & PB_BATCH_ASYNC) return PB_OK;

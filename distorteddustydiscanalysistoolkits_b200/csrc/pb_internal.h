@@ -17,6 +17,8 @@ struct BatchDisc {
     DevCatalog C32, C64;
     const float4 *pay;
     const double *qx, *qy, *qz;
+    const int2 *cut;     // the disc's walk cut (subtree root, node after it), in DFS order
+    const int *ncut;     // its number of subtrees (device-resident: the cut is made on the device)
     int64_t nq;
     int stride;
     int pad;
@@ -113,6 +115,9 @@ struct Handle {
     int batch_order = 0;     // 0: discs in the given order, 1: discs with the most work first
     int batch_blocks = 0;    // blocks per SM of the batched pair kernel (0: as many as fit)
     int64_t batch_slice = 0; // sample points per slice the batch's run pool was sized for
+    int batch_ns = 0;        // subtrees per point the batch's item records were sized for
+    int batch_walk_split = 16;   // target number of subtrees per disc of the batched walk
+    DBuf batch_slot_of;      // processing slot of every point of a slice
 
     // query-side scratch
     DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
@@ -148,6 +153,8 @@ cudaError_t launch_permute_back(Handle *H, int64_t n, const uint32_t *idx, const
 
 // ---- launchers (pb_walk.cu) ----
 cudaError_t launch_cut(Handle *H, const DevTree &T, int target, int *ns_out);
+// launch_cut without the read-back: the ordered cut and its size stay on the device
+cudaError_t launch_cut_device(Handle *H, const DevTree &T, int target, const int2 **cut, const int **count);
 cudaError_t launch_nearest_list(Handle *H, const DevTree &T, int64_t m, const uint32_t *ql, const double *qx,
                                 const double *qy, const double *qz, int *bnear);
 cudaError_t launch_walk(Handle *H, const DevTree &T, int strategy, const RunPool &P, int64_t m, const uint32_t *ql,
@@ -211,7 +218,7 @@ struct LineFrame {
 cudaError_t launch_batch_slice(Handle *H, int strategy, int kernel, int cat, const BatchDisc *discs,
                                const int64_t *starts, const uint32_t *slot_disc, int ndisc, int64_t s0, int64_t m,
                                const RunPool &P, int fp64_only, unsigned light_max, int leaf_size, int blocks_per_sm,
-                               unsigned long long *ctr);
+                               int *slot_of, unsigned long long *ctr);
 cudaError_t launch_batch_payload(Handle *H, const DevTree &T, const DevCatalog &C, float4 **pay, int *stride);
 cudaError_t launch_line_image(Handle *H, const double *a0, int64_t n0, const double *a1, int64_t n1, const LineFrame &F,
                               double *ox, double *oy, double *oz, double *dx, double *dy, double *dz);

@@ -257,6 +257,27 @@ cudaError_t launch_cut(Handle *H, const DevTree &T, int target, int *ns_out)
     return cudaSuccess;
 }
 
+cudaError_t launch_cut_device(Handle *H, const DevTree &T, int target, const int2 **cut, const int **count)
+{
+    const int64_t n = T.n;
+    int64_t tsz = (n + target - 1) / target;
+    if (tsz < 1) tsz = 1;
+    const int cap = 4 * target + 8;
+    cudaError_t e;
+    if ((e = H->cut.reserve(sizeof(int2) * 2 * cap + 16))) return e;
+    int2 *raw = H->cut.as<int2>();
+    int2 *sorted = raw + cap;
+    int *cnt = reinterpret_cast<int *>(raw + 2 * cap);
+    if ((e = cudaMemsetAsync(cnt, 0, sizeof(int), H->stream))) return e;
+    const int64_t ntot = T.root ? 2 * n - 1 : 1;
+    k_cut_mark<<<grid_for(ntot, 256), 256, 0, H->stream>>>(T, H->parent.as<int>(), tsz, raw, cnt, cap);
+    k_cut_order<<<1, 1024, 0, H->stream>>>(T, raw, cnt, cap, sorted);
+    H->launches += 2;
+    *cut = sorted;
+    *count = cnt;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nearest_list(Handle *H, const DevTree &T, int64_t m, const uint32_t *ql, const double *qx,
                                 const double *qy, const double *qz, int *bnear)
 {

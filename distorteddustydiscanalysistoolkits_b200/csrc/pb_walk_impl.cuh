@@ -63,11 +63,12 @@ struct RunWriter {
     __device__ __forceinline__ bool close(const RunPool &P) { return olo < 0 || store(P); }
 };
 
-// One (query, subtree) item: walk subtree s for the j-th listed query (sample point qi at
-// px, py, pz; nearest sorted leaf P.bnear[j]) and write its runs.
+// One (query, subtree) item: walk subtree s of the cut `cut` (P.cut for a single tree) for the
+// j-th listed query (sample point qi at px, py, pz; nearest sorted leaf P.bnear[j]) and write
+// its runs.
 template <int STRAT>
-__device__ __forceinline__ void walk_item_at(const DevTree &T, const RunPool &P, int64_t j, int s, uint32_t qi,
-                                             double px, double py, double pz, double K)
+__device__ __forceinline__ void walk_item_at(const DevTree &T, const RunPool &P, const int2 *__restrict__ cut,
+                                             int64_t j, int s, uint32_t qi, double px, double py, double pz, double K)
 {
     bool ok = P.count_only || (*(volatile unsigned long long *)P.used < P.cap &&
                                *(volatile int *)(P.qflag + j) == 0);   // pool exhausted or query deferred
@@ -84,7 +85,7 @@ __device__ __forceinline__ void walk_item_at(const DevTree &T, const RunPool &P,
             double d2;
             if (single_leaf_accepted<STRAT>(T, px, py, pz, K, r2a, L, d2)) ok = R.emit(P, 0, 0);
         } else {
-            const int2 c = __ldg(P.cut + s);
+            const int2 c = __ldg(cut + s);
             auto emit = [&](int64_t lo, int64_t hi) { return R.emit(P, lo, hi); };
             ok = walk_subtree<STRAT>(T, c.x, c.y, px, py, pz, K, r2a, emit, P.leaf_size);
         }
@@ -113,7 +114,7 @@ __device__ __forceinline__ void walk_item(const DevTree &T, const RunPool &P, in
                                           const double *__restrict__ qy, const double *__restrict__ qz, double K)
 {
     const uint32_t qi = __ldg(ql + j);
-    walk_item_at<STRAT>(T, P, j, s, qi, __ldg(qx + qi), __ldg(qy + qi), __ldg(qz + qi), K);
+    walk_item_at<STRAT>(T, P, P.cut, j, s, qi, __ldg(qx + qi), __ldg(qy + qi), __ldg(qz + qi), K);
 }
 
 }  // namespace pb

@@ -172,13 +172,15 @@ int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb
    snapshot per call, PointSamples_interpolation.jl:12-29; this batches calls).  discs[k] is a
    handle on which pb_linear_bvh has built disc k (PB_BUILD_ASYNC allowed); npts[k] sample
    points at qx[k], qy[k], qz[k] and the L = n_scalar + 3 n_grad + n_div + 3 n_curl outputs
-   out[k * L + l] are device memory.  One persistent kernel sums every disc's points (FP64: the
-   reference's arithmetic; FP32C: queries with at most fp64_light_max neighbours in FP64, the
-   rest FP32-compensated, decided on the device), with values equal to separate
-   pb_interpolate_points calls bit for bit.  Every handle must use the first one's device,
-   stream (pb_set_stream) and kernel; the catalog must fit one launch.  Options of discs[0]:
-   "leaf_size" (walk cutoff), "batch_order" (0 given, 1 most work first) and
-   "batch_blocks_per_sm" (0 = all that fit) change the schedule only.  With device pointers, no
+   out[k * L + l] are device memory.  Every disc's tree is cut into subtrees on the device; one
+   walk launch covers every disc's (point, subtree) items and persistent kernels sum every
+   disc's points (FP64: the reference's arithmetic; FP32C: queries with at most fp64_light_max
+   neighbours in FP64, the rest FP32-compensated, decided on the device), with values equal to
+   separate pb_interpolate_points calls bit for bit.  Every handle must use the first one's
+   device, stream (pb_set_stream) and kernel; the catalog must fit one launch.  Options of
+   discs[0]: "leaf_size" (walk cutoff), "batch_walk_split" (target subtrees per disc, 1..1024,
+   default 16), "batch_order" (0 given, 1 most work first) and "batch_blocks_per_sm" (0 = all
+   that fit) change the schedule only.  With device pointers, no
    synchronisation and all buffers already sized by an earlier identical call, the builds with
    PB_BUILD_ASYNC and this call with PB_BATCH_ASYNC can be captured in a CUDA graph. */
 int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalog *cat, const int64_t *npts,
