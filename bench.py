@@ -481,7 +481,7 @@ def run_c4(args, rank, world):
         if step >= args.warmup:
             res_ms.append(tot)
     hd.set_option("timing", 0)
-    tuner = batch.BatchAutotuner(leaf_size=(1, 8), order=(0, 1), blocks_per_sm=(0,), walk_split=(8, 16, 32),
+    tuner = batch.BatchAutotuner(leaf_size=(1, 8), order=(0, 1), blocks_per_sm=(0,), walk_split=(16, 32, 64),
                                  repeats=1)
     best = tuner.tune(db)
     db.timed(args.warmup)

@@ -684,26 +684,53 @@ cudaError_t launch_topology(Handle *H, int64_t n)
 
 // ------------------------------------------------------------------------------------
 // Morton order of query points (schedule only: outputs are written back to their own slot)
+// 30-bit Morton code of a sample point in a tree's quantisation frame (10 bits per axis,
+// clamped to the particles' box): only an ordering key, not the build's codes
+__device__ __forceinline__ uint32_t query_code30(const QuantParams &q, double x, double y, double z)
+{
+    const double p[3] = {x, y, z};
+    uint32_t c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double f = q.flat[d] ? 0.5 : (p[d] - q.vmin[d]) * q.inv[d];
+        f = fmin(fmax(f, 0.0), 1.0);
+        if (!(f == f)) f = 0.0;
+        c[d] = (uint32_t)(f * 1023.0);
+    }
+    return ((uint32_t)expand_bits3(c[0]) << 2) | ((uint32_t)expand_bits3(c[1]) << 1) | (uint32_t)expand_bits3(c[2]);
+}
+
 __global__ void k_query_codes(int64_t nq, const double *__restrict__ qx, const double *__restrict__ qy,
                               const double *__restrict__ qz, const QuantParams *__restrict__ qp, uint32_t *keys,
                               uint32_t *perm)
 {
-    QuantParams q = *qp;
+    const QuantParams q = *qp;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nq; i += (int64_t)gridDim.x * blockDim.x) {
-        double p[3] = {qx[i], qy[i], qz[i]};
-        uint32_t c[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double f = q.flat[d] ? 0.5 : (p[d] - q.vmin[d]) * q.inv[d];
-            f = fmin(fmax(f, 0.0), 1.0);
-            if (!(f == f)) f = 0.0;
-            c[d] = (uint32_t)(f * 1023.0);
-        }
-        uint32_t code = ((uint32_t)expand_bits3(c[0]) << 2) | ((uint32_t)expand_bits3(c[1]) << 1) |
-                        (uint32_t)expand_bits3(c[2]);
-        keys[i] = code;
+        keys[i] = query_code30(q, qx[i], qy[i], qz[i]);
         perm[i] = (uint32_t)i;
     }
+}
+
+__global__ void k_batch_query_codes(int64_t m, const BatchDisc *__restrict__ discs, const int64_t *__restrict__ starts,
+                                    const uint32_t *__restrict__ slot_disc, const int *__restrict__ slot_of,
+                                    int64_t s0, uint64_t *keys, uint32_t *vals)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+        const int lo = slot_of[t];
+        const BatchDisc &D = discs[slot_disc[lo]];
+        const int64_t qi = s0 + t - starts[lo];
+        keys[t] = ((uint64_t)(uint32_t)lo << 32) | query_code30(*D.qp, D.qx[qi], D.qy[qi], D.qz[qi]);
+        vals[t] = (uint32_t)t;
+    }
+}
+
+cudaError_t launch_batch_query_codes(Handle *H, int64_t m, const BatchDisc *discs, const int64_t *starts,
+                                     const uint32_t *slot_disc, const int *slot_of, int64_t s0, uint64_t *keys,
+                                     uint32_t *vals)
+{
+    k_batch_query_codes<<<grid_for(m, 256), 256, 0, H->stream>>>(m, discs, starts, slot_disc, slot_of, s0, keys, vals);
+    H->launches += 1;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_query_codes(Handle *H, int64_t nq, const double *qx, const double *qy, const double *qz,

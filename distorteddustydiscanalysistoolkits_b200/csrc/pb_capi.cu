@@ -101,6 +101,7 @@ int check_status(Handle &H)
     if (st & ST_TRAVERSAL) return fail(H, PB_ERR_INTERNAL, "traversal exceeded its iteration bound");
     if (st & ST_POOL)
         return fail(H, PB_ERR_DIMENSION, "neighbour pool offsets too small for a query (DimensionMismatch)");
+    if (st & ST_CUT) return fail(H, PB_ERR_INTERNAL, "walk cut larger than its capacity (raise batch_walk_split)");
     return PB_OK;
 }
 
@@ -1529,6 +1530,7 @@ int32_t pb_batch_points(pb_handle *const *discs, int32_t ndiscs, const pb_catalo
         D.nq = npts[k];
         // the disc's walk cut, made on the device from the tree just built
         CK(launch_cut_device(&Hk, D.T, H.batch_walk_split, &D.cut, &D.ncut));
+        D.qp = Hk.qparams.as<QuantParams>();
         if (precision == PB_FP32C) {
             float4 *pay = nullptr;
             int stride = 0;

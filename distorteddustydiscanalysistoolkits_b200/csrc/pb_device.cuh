@@ -33,6 +33,7 @@ constexpr int ST_NONFINITE = 1;     // non-finite particle coordinate or smoothi
 constexpr int ST_REFIT = 2;         // an internal node was not combined exactly twice
 constexpr int ST_TRAVERSAL = 4;     // a traversal exceeded its iteration bound (corrupt tree)
 constexpr int ST_POOL = 8;          // neighbour pool too small for a query
+constexpr int ST_CUT = 16;          // a walk cut made on the device had more subtrees than its capacity
 
 struct __align__(16) NodeF {
     float lox, loy, loz;

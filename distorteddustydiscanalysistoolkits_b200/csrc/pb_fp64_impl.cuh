@@ -161,13 +161,10 @@ __device__ __forceinline__ void pairs64_query(const DevTree &T, const DevCatalog
     };
     auto first = [&](int64_t) {};
     auto one = [&](int64_t b) { proc(32, b); };
-    auto two = [&](int64_t m1) {
-        proc(32, m1);
-        proc(32, m1 + 32);
-    };
     auto cantwo = [&]() { return false; };
-    // never called (canfour is false): an empty body keeps the kernels free of a stack frame,
-    // which a four-batch body here would force on the per-pair term array
+    // never called (cantwo and canfour are false): empty bodies keep the kernels free of a
+    // stack frame, which a multi-batch body here would force on the per-pair term array
+    auto two = [&](int64_t) {};
     auto four = [&](int64_t) {};
     int mine = -1;
     const int fill = deal_runs(P, j, lane, first, one, two, cantwo, four, cantwo, mine);

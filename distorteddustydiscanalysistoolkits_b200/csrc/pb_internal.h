@@ -12,6 +12,8 @@ namespace pb {
 
 // One disc of a batched launch (pb_batch.cu): its tree, the FP32C and FP64 catalogs of its
 // columns and outputs, its FP32C payload, and its sample points.
+struct QuantParams;
+
 struct BatchDisc {
     DevTree T;
     DevCatalog C32, C64;
@@ -19,6 +21,7 @@ struct BatchDisc {
     const double *qx, *qy, *qz;
     const int2 *cut;     // the disc's walk cut (subtree root, node after it), in DFS order
     const int *ncut;     // its number of subtrees (device-resident: the cut is made on the device)
+    const QuantParams *qp;   // the disc's quantisation frame (Morton order of its sample points)
     int64_t nq;
     int stride;
     int pad;
@@ -118,6 +121,8 @@ struct Handle {
     int batch_ns = 0;        // subtrees per point the batch's item records were sized for
     int batch_walk_split = 16;   // target number of subtrees per disc of the batched walk
     DBuf batch_slot_of;      // processing slot of every point of a slice
+    DBuf batch_bcnt, batch_boff, batch_bcur, batch_list;   // walk prefilter: buckets and item list
+    DBuf batch_mk, batch_mka, batch_mv, batch_mva;         // Morton walk order of a slice
 
     // query-side scratch
     DBuf q_x, q_y, q_z, q_keys, q_keys_alt, q_perm, q_perm_alt, q_out, q_aux;
@@ -143,6 +148,11 @@ cudaError_t sort_pairs_u64(Handle *H, uint64_t *keys, uint32_t *vals, uint64_t *
 cudaError_t sort_pairs_u32(Handle *H, uint32_t *keys, uint32_t *vals, uint32_t *kalt, uint32_t *valt, int64_t n,
                            int bits);
 cudaError_t launch_exclusive_scan_u32(Handle *H, const uint32_t *in, uint32_t *out, int64_t m);
+// per point t of a batch slice: key (processing slot << 32) | Morton code of the point in its
+// disc's quantisation frame, value t
+cudaError_t launch_batch_query_codes(Handle *H, int64_t m, const BatchDisc *discs, const int64_t *starts,
+                                     const uint32_t *slot_disc, const int *slot_of, int64_t s0, uint64_t *keys,
+                                     uint32_t *vals);
 cudaError_t launch_dedupe(Handle *H, uint64_t *codes, int64_t n);
 cudaError_t launch_gather(Handle *H, int64_t n, const double *x, const double *y, const double *z, const double *h,
                           const double *m, const double *rho, const std::vector<const double *> &cols);

@@ -257,6 +257,13 @@ cudaError_t launch_cut(Handle *H, const DevTree &T, int target, int *ns_out)
     return cudaSuccess;
 }
 
+// a device-made cut that overflowed its capacity flags the tree's status word (the host
+// path returns an error instead)
+__global__ void k_cut_check(const int *count, int cap, int *status)
+{
+    if (*count > cap) atomicOr(status, ST_CUT);
+}
+
 cudaError_t launch_cut_device(Handle *H, const DevTree &T, int target, const int2 **cut, const int **count)
 {
     const int64_t n = T.n;
@@ -272,7 +279,8 @@ cudaError_t launch_cut_device(Handle *H, const DevTree &T, int target, const int
     const int64_t ntot = T.root ? 2 * n - 1 : 1;
     k_cut_mark<<<grid_for(ntot, 256), 256, 0, H->stream>>>(T, H->parent.as<int>(), tsz, raw, cnt, cap);
     k_cut_order<<<1, 1024, 0, H->stream>>>(T, raw, cnt, cap, sorted);
-    H->launches += 2;
+    k_cut_check<<<1, 1, 0, H->stream>>>(cnt, cap, T.status);
+    H->launches += 3;
     *cut = sorted;
     *count = cnt;
     return cudaGetLastError();
