@@ -77,14 +77,15 @@ __device__ __forceinline__ float ldexp_norm3(int k)
 }
 
 // payload: record of `stride` float4 fields per sorted particle
-//   [0] = {x_hi, y_hi, z_hi, 1/h}, [1] = {x_lo, y_lo, z_lo, m/rho}, [2] = {sigma h^-3, sigma h^-4, A0_hi, A0_lo},
-//   [3..] = remaining (hi, lo) column pairs.  Coordinates are double-float pairs, so the pair
+//   [0] = {x_hi, y_hi, z_hi, 1/h}, [1] = {x_lo, y_lo, z_lo, m/rho}, [2..] = the (hi, lo) pairs of the
+//   columns, two per field (64 bytes for four columns).  The kernel factors sigma h^-3 and
+//   sigma h^-4 are formed from 1/h in the pair loop: four multiplies cost less than the load.  Coordinates are double-float pairs, so the pair
 //   offset x_a - x_b is formed in FP32 as (xa_hi - xb_hi) + (xa_lo - xb_lo) without FP64 loads.
 // Layout: blocks of 32 consecutive particles, field-major inside a block -- field k of particle
 // b is float4 number ((b / 32) * stride + k) * 32 + b % 32.  The lanes of a warp read 32
 // consecutive particles (the common case: a batch inside one accepted run), so every field
 // load of the warp is one contiguous 512-byte segment.
-__host__ __device__ inline int payload_stride(int nU) { return 2 + (2 + 2 * nU + 3) / 4; }
+__host__ __device__ inline int payload_stride(int nU) { return 2 + (2 * nU + 3) / 4; }
 constexpr int PAY_BLOCK = 32;   // particles per payload block; field k is at rec[k * PAY_BLOCK]
 
 __host__ __device__ inline int64_t payload_float4s(int64_t n, int stride)
@@ -125,7 +126,7 @@ struct CatShape {
     __device__ static __forceinline__ bool any(const DevCatalog &C) { return grad(C) || div(C) || curl(C); }
     __device__ static __forceinline__ int stride(int s)
     {
-        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 5 : ((CAT == CAT_S1 || CAT == CAT_SG1) ? 3 : s);
+        return (CAT == CAT_GDC4 || CAT == CAT_C4) ? 4 : ((CAT == CAT_S1 || CAT == CAT_SG1) ? 3 : s);
     }
 };
 
@@ -141,7 +142,6 @@ inline int catalog_shape(const DevCatalog &C)
 // internal linkage: each unit that includes this header gets its own copy of the kernel
 static __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay, int stride)
 {
-    const float sig = ldexp_norm3(T.kernel);
     for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x) {
         double4 L = T.leaf[b];
         double ih = 1.0 / L.w;
@@ -150,18 +150,15 @@ static __global__ void k_payload(int64_t n, DevTree T, DevCatalog C, float4 *pay
         rec[0] = make_float4(xh, yh, zh, (float)ih);
         rec[PAY_BLOCK] = make_float4((float)(L.x - (double)xh), (float)(L.y - (double)yh), (float)(L.z - (double)zh),
                                      (float)(T.m[b] / T.rho[b]));
-        float v[2 + 2 * MAXU + 2];
-        v[0] = (float)(sig * ih * ih * ih);
-        v[1] = (float)(sig * ih * ih * ih * ih);
+        float v[2 * MAXU + 4];
 #pragma unroll
         for (int u = 0; u < MAXU; ++u) {
             double a = (u < C.nU) ? C.ucol[u][b] : 0.0;
             float hi = (float)a;
-            v[2 + 2 * u] = hi;
-            v[3 + 2 * u] = (float)(a - (double)hi);
+            v[2 * u] = hi;
+            v[2 * u + 1] = (float)(a - (double)hi);
         }
-        v[2 + 2 * MAXU] = 0.f;
-        v[3 + 2 * MAXU] = 0.f;
+        v[2 * MAXU] = v[2 * MAXU + 1] = v[2 * MAXU + 2] = v[2 * MAXU + 3] = 0.f;
         for (int k = 2; k < stride; ++k)
             rec[k * PAY_BLOCK] = make_float4(v[4 * k - 8], v[4 * k - 7], v[4 * k - 6], v[4 * k - 5]);
     }
@@ -232,25 +229,23 @@ struct Acc32 {
 };
 
 struct Query32 {
-    float ih, cw, cg;   // 1/h_a, sigma h_a^-3, sigma h_a^-4
+    float ih, cw, cg, sig;   // 1/h_a, sigma h_a^-3, sigma h_a^-4, sigma
     float ph[3], pl[3]; // query position as double-float pairs
 };
 
-// kernel constants and column value pairs (hi, lo) of a record
+// column value pairs (hi, lo) of a record
 template <int CAT>
-__device__ __forceinline__ void load_cols(const float4 *rec, int stride, float &cW, float &cG, float *ch, float *cl)
+__device__ __forceinline__ void load_cols(const float4 *rec, int stride, float *ch, float *cl)
 {
     stride = CatShape<CAT>::stride(stride);
-    float v[4 * 4];
+    float v[8];
 #pragma unroll
-    for (int k = 2; k < 6; ++k) {
+    for (int k = 2; k < 4; ++k) {
         float4 c = (k < stride) ? __ldg(rec + k * PAY_BLOCK) : make_float4(0.f, 0.f, 0.f, 0.f);
         v[4 * k - 8] = c.x; v[4 * k - 7] = c.y; v[4 * k - 6] = c.z; v[4 * k - 5] = c.w;
     }
-    cW = v[0];
-    cG = v[1];
 #pragma unroll
-    for (int u = 0; u < MAXU; ++u) { ch[u] = v[2 + 2 * u]; cl[u] = v[3 + 2 * u]; }
+    for (int u = 0; u < MAXU; ++u) { ch[u] = v[2 * u]; cl[u] = v[2 * u + 1]; }
 }
 
 // per-pair terms: weight m_b/rho_b W, quantity offsets a_u, weighted kernel gradient
@@ -269,8 +264,9 @@ __device__ __forceinline__ void terms32(const Acc32 &A, const DevCatalog &C, con
     const float dx = (Q.ph[0] - p0.x) + (Q.pl[0] - p1.x);
     const float dy = (Q.ph[1] - p0.y) + (Q.pl[1] - p1.y);
     const float dz = (Q.ph[2] - p0.z) + (Q.pl[2] - p1.z);
-    float cWb, cGb, ch[MAXU], cl[MAXU];
-    load_cols<CAT>(rec, stride, cWb, cGb, ch, cl);
+    float ch[MAXU], cl[MAXU];
+    load_cols<CAT>(rec, stride, ch, cl);
+    const float cWb = ((Q.sig * p0.w) * p0.w) * p0.w, cGb = cWb * p0.w;
     const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
     // the SFU's reciprocal square root without the subnormal-input path of rsqrtf (the
     // approximation is the same for normal inputs); a pair closer than 1e-15 (r2 <= 1e-30)
@@ -415,6 +411,7 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
                                         Query32 &Q, Acc32 &A, const float4 *pay, int stride, double *slots)
 {
     Q = Query32{};
+    Q.sig = sig;
     if (STRAT != SCATTER) {
         double ha = bnear < 0 ? __longlong_as_double(0x7ff8000000000000LL) : ldg4(T.leaf + bnear).w;
         float ih = (float)(1.0 / ha);
@@ -429,8 +426,7 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
     if (bnear >= 0) {
         // quantities enter as offsets from the nearest particle's values, which are close
         // to the kernel-weighted means, so gradient/divergence/curl sums cancel far less
-        float cw_, cg_;
-        load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), (uint32_t)bnear), stride, cw_, cg_, A.hh, A.hl);
+        load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), (uint32_t)bnear), stride, A.hh, A.hl);
         A.have = true;
     }
 }
@@ -438,8 +434,7 @@ __device__ __forceinline__ void setup32(const DevTree &T, float sig, double px, 
 template <int CAT>
 __device__ __forceinline__ void offsets_from(Acc32 &A, const float4 *pay, int stride, int b0)
 {
-    float cw_, cg_;
-    load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), b0), stride, cw_, cg_, A.hh, A.hl);
+    load_cols<CAT>(rec_of(pay, CatShape<CAT>::stride(stride), b0), stride, A.hh, A.hl);
     A.have = true;
 }
 
