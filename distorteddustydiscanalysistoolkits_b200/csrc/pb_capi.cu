@@ -497,6 +497,10 @@ int reserve_pool(Handle &H, int64_t m, int ns)
     unsigned long long cap = budget / per_chunk;
     if (cap > want) cap = want;
     if (env_mb <= 0 && cap < min_chunks) cap = min_chunks;
+    // a pool an earlier call grew (grow_pool) is kept: its memory is already held
+    const unsigned long long held = std::min<unsigned long long>(H.pool_runs.bytes / (sizeof(uint2) * RUN_CHUNK),
+                                                                 H.pool_next.bytes / sizeof(int));
+    if (env_mb <= 0 && held > cap) cap = held;
     if (env_chunks > 0) cap = (unsigned long long)env_chunks;
     if (cap < 1) cap = 1;
     if (cap > 0x7fffffffULL) cap = 0x7fffffffULL;
@@ -650,7 +654,12 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
     H.walk_rounds = 0;
     H.deferred_total = 0;
     for (int k = 0; k < 3; ++k) H.t_phase_ms[k] = 0.f;
-    int64_t Snext = S;   // slice size, adapted to the pool use seen so far
+    // slice size, adapted to the pool use seen so far; the first slice is sized from the largest
+    // per-query pool use of the handle's previous call, when there was one
+    int64_t Snext = S;
+    if (H.pool_cpq > 0.0)
+        Snext = std::max<int64_t>(1024, std::min<int64_t>(S, (int64_t)(0.85 * (double)H.pool_cap / H.pool_cpq)));
+    double cpq_max = 0.0;
     for (int64_t s0 = 0; s0 < npts;) {
         const uint32_t *ql = ql_all + s0;
         int64_t m = std::min<int64_t>(Snext, npts - s0);
@@ -730,6 +739,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
                 const int64_t done = m - (int64_t)nd;
                 if (done > 0 && used > 0) {
                     const double per = (double)used / (double)done;
+                    cpq_max = std::max(cpq_max, per);
                     Snext = std::max<int64_t>(1024, std::min<int64_t>(S, (int64_t)(0.85 * (double)H.pool_cap / per)));
                 } else if (nd > 0) {
                     Snext = std::max<int64_t>(1024, Snext / 2);
@@ -762,6 +772,7 @@ int two_phase_points(Handle &H, const DevTree &T, const std::vector<Launch> &lau
             m = nd;
         }
     }
+    if (cpq_max > 0.0) H.pool_cpq = cpq_max;
     return PB_OK;
 }
 

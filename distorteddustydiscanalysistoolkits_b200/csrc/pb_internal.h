@@ -98,6 +98,7 @@ struct Handle {
     int sched = 1;         // 0 plain (input order, one walk per query, no ordering), 1 tuned, 2 learned
     int64_t light_max = 4096;   // FP32C: queries with at most this many neighbours are summed in FP64
     int64_t slice = int64_t(1) << 22;   // queries per two-phase slice
+    double pool_cpq = 0.0;   // largest pool chunks per completed query seen by the last call (0: none)
     // learned work prediction (pb_sched.cu)
     DBuf mlp_w, mlp_m, mlp_v, mlp_g, mlp_norm, mlp_scr, mlp_idx, mlp_x, mlp_y, mlp_loss, sched_feat, sched_pred,
         sched_ql, sched_tmp;
