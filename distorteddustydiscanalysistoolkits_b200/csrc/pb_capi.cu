@@ -860,16 +860,17 @@ int do_lines(Handle &H, const pb_catalog *cat, int64_t nl, const double *ox, con
     std::vector<int> is_host;
     if ((rc = stage_outputs(H, L, nl, out, dev, is_host))) return rc;
     DevTree T = make_tree(H);
-    std::vector<Launch> launches = plan(items_of(cat, precision == PB_FP32C));
+    // Both precision modes take the FP64 line kernel.  An FP32-compensated line sum needs its
+    // projected distances and table indices in FP64 too (FP32 ones miss the 1e-5 tolerance on
+    // 256^2 images), so only its accumulation would be cheaper, and that did not pay: the whole
+    // C3 image took 433 ms with FP32C accumulation against 388 ms in FP64.
+    std::vector<Launch> launches = plan(items_of(cat, false));
     ev_record(H, 2);   // the line ordering is part of the timed interpolation
     const uint32_t *perm;
     if ((rc = query_order(H, nl, dox, doy, doz, &perm))) return rc;
     for (const Launch &Lc : launches) {
         DevCatalog C = dev_catalog(H, Lc, dev.data());
-        if (precision == PB_FP64)
-            CK(launch_lines_fp64(&H, T, C, nl, dox, doy, doz, (const double *)a, (const double *)b, (const double *)c, perm));
-        else
-            CK(launch_lines_fp32(&H, T, C, nl, dox, doy, doz, (const double *)a, (const double *)b, (const double *)c, perm));
+        CK(launch_lines_fp64(&H, T, C, nl, dox, doy, doz, (const double *)a, (const double *)b, (const double *)c, perm));
         H.interp_launches++;
     }
     ev_record(H, 3);

@@ -210,9 +210,6 @@ cudaError_t launch_points_fp32(Handle *H, const DevTree &T, const DevCatalog &C,
 cudaError_t launch_lines_fp64(Handle *H, const DevTree &T, const DevCatalog &C, int64_t nl, const double *ox,
                               const double *oy, const double *oz, const double *dx, const double *dy,
                               const double *dz, const uint32_t *perm);
-cudaError_t launch_lines_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int64_t nl, const double *ox,
-                              const double *oy, const double *oz, const double *dx, const double *dy,
-                              const double *dz, const uint32_t *perm);
 cudaError_t launch_nearest(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,
                            const double *qz, double *h_out, int64_t *idx_out);
 cudaError_t launch_query(Handle *H, const DevTree &T, int64_t nq, const double *qx, const double *qy,

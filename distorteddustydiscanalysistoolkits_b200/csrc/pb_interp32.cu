@@ -4,25 +4,24 @@
 // per-leaf acceptance test run in FP64 exactly as there, and accepted neighbours are
 // processed in the same DFS order.  Per pair, the kernel values and the accumulated terms
 // are FP32:
-//   * a per-call particle payload (built once per launch) holds 1/h_b, sigma h_b^-3,
-//     sigma h_b^-4, m_b/rho_b and every quantity column as a (hi, lo) float pair, so the
-//     pair needs no division and no FP64 column arithmetic;
-//   * kernel shapes are evaluated branch-free from their truncated-power forms
-//     (M4: 0.25 (2-q)_+^3 - (1-q)_+^3, ...), templated on the kernel type;
+//   * a per-call particle payload (built once per launch) holds the position as double-float
+//     pairs, 1/h_b, m_b/rho_b and every quantity column as a (hi, lo) float pair, so the pair
+//     needs no division and no FP64 column arithmetic (sigma h_b^-3 and sigma h_b^-4 are
+//     formed from 1/h_b);
+//   * kernel shapes are evaluated branch-free (selects between pieces written so that nothing
+//     cancels near q = 0), templated on the kernel type;
 //   * every quantity enters as an offset A_b - A_hat (A_hat = the nearest particle's value,
 //     or the first accepted neighbour's for scatter, as a double-float) so that
 //     gradient/divergence/curl F - A B cancels as little as possible;
-//   * each lane sums its terms in plain FP32 over chunks of 16 full batches of 32 pairs (16 of
+//   * each lane sums its terms in plain FP32 over chunks of 32 full batches of 32 pairs (32 of
 //     its own pairs) and adds each chunk sum, converted exactly, to an FP64 accumulator.
+// Line integrals are not here: both precision modes use the FP64 line kernel (pb_interp64.cu).
 // The per-query arithmetic depends only on the query and the tree (chunks are counted over
 // the query's own accepted-neighbour sequence), never on the launch shape or schedule.
-#include "line_tables.h"
 #include "pb_internal.h"
 #include "pb_fp32_impl.cuh"
 
 namespace pb {
-
-__device__ const float g_line_inorm32[6][PB_LINE_NTAB] = PB_LINE_INORM_INIT;
 
 // Fused form: the warp walks the query's tree itself (warp-uniform next_item) and deals the
 // accepted leaves to its lanes.  Used for queries the run pool could not hold.
@@ -187,19 +186,6 @@ cudaError_t launch_pairs_fp32(Handle *H, const DevTree &T, const DevCatalog &C, 
     default: launch_pairs_kt<SYMMETRIC>(H, T, C, pay, stride, P, m, ql, order, qx, qy, qz, ctr); break;
     }
     H->launches += 2;
-    return cudaGetLastError();
-}
-
-cudaError_t launch_lines_fp32(Handle *H, const DevTree &T, const DevCatalog &C, int64_t nl, const double *ox,
-                              const double *oy, const double *oz, const double *dx, const double *dy,
-                              const double *dz, const uint32_t *perm)
-{
-    const float *tab = nullptr;
-    cudaError_t e = cudaGetSymbolAddress((void **)&tab, g_line_inorm32);
-    if (e) return e;
-    int bs = 128;
-    k_lines<float><<<grid_for(nl, bs, 1 << 30), bs, 0, H->stream>>>(T, C, nl, ox, oy, oz, dx, dy, dz, perm, tab);
-    H->launches += 1;
     return cudaGetLastError();
 }
 
