@@ -162,7 +162,8 @@ int32_t pb_point_samples_interpolation(pb_handle *h, const pb_input *in, const p
                                        int32_t precision, double *const *out, int32_t flags);
 
 /* Partia.LineSamples_interpolation(::CUDAComputeBackend, lines, input, catalog, itpScatter)
-   (Partia.jl/ext/CUDAExt/KernelInterpolation/grid_interpolation/LineSamples_interpolation.jl:11-34). */
+   (Partia.jl/ext/CUDAExt/KernelInterpolation/grid_interpolation/LineSamples_interpolation.jl:11-34).
+   Both precision modes sum the line integrals in FP64 (the reference's arithmetic). */
 int32_t pb_line_samples_interpolation(pb_handle *h, const pb_input *in, const pb_catalog *cat, int64_t nlines,
                                       const double *ox, const double *oy, const double *oz, const double *dx,
                                       const double *dy, const double *dz, int32_t strategy, int32_t precision,
