@@ -264,9 +264,12 @@ __global__ void __launch_bounds__(128) k_batch_pairs64(const BatchDisc *__restri
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t first = *O.nheavy, end = m - (int64_t)*O.nover;
     DescCache dc;
-    for (;;) {
-        const int64_t pos = first + next_query(counter, lane);
-        if (pos >= end) break;
+    // the next point's position is fetched while the current one is summed (k_pairs64w)
+    unsigned long long nxt = 0;
+    if (lane == 0) nxt = atomicAdd(counter, 1ULL);
+    int64_t pos = first + (int64_t)__shfl_sync(0xffffffffu, nxt, 0);
+    for (; pos < end; pos = first + (int64_t)__shfl_sync(0xffffffffu, nxt, 0)) {
+        if (lane == 0) nxt = atomicAdd(counter, 1ULL);
         const int64_t t = __ldg(O.ord + pos), j = s0 + t;
         const int lo = __ldg(O.slot_of + t);
         const BatchDisc &D = dc.get(discs, s_desc[wib], (int)__ldg(slot_disc + lo), lane);

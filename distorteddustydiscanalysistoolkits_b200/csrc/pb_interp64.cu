@@ -40,15 +40,22 @@ __global__ void __launch_bounds__(128) k_pairs64w(DevTree T, DevCatalog C, RunPo
 {
     __shared__ double sterm[4][32][NT + 1];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    for (;;) {
-        int64_t t = next_query(counter, lane);
-        if (t >= m) break;
+    // the next query's position in the order is fetched (lane 0's atomic) while the current
+    // one is summed, so the counter's latency overlaps the work; which warp sums a query does
+    // not change its value
+    unsigned long long nxt = 0;
+    if (lane == 0) nxt = atomicAdd(counter, 1ULL);
+    int64_t t = (int64_t)__shfl_sync(0xffffffffu, nxt, 0);
+    while (t < m) {
+        if (lane == 0) nxt = atomicAdd(counter, 1ULL);
         const int64_t j = order ? (int64_t)__ldg(order + t) : t;
-        if (__ldg(P.qflag + j)) continue;
-        const int64_t qi = __ldg(ql + j);
-        const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
-        pairs64_query<STRAT>(T, C, P, j, qi, px, py, pz, STRAT != SCATTER ? (int64_t)__ldg(P.bnear + j) : -1,
-                             &sterm[wib][0][0], lane);
+        if (!__ldg(P.qflag + j)) {
+            const int64_t qi = __ldg(ql + j);
+            const double px = __ldg(qx + qi), py = __ldg(qy + qi), pz = __ldg(qz + qi);
+            pairs64_query<STRAT>(T, C, P, j, qi, px, py, pz, STRAT != SCATTER ? (int64_t)__ldg(P.bnear + j) : -1,
+                                 &sterm[wib][0][0], lane);
+        }
+        t = (int64_t)__shfl_sync(0xffffffffu, nxt, 0);
     }
 }
 
