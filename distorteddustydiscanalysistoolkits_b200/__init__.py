@@ -5,6 +5,8 @@ include/partia_b200.h).  This package is the host-side mirror of Partia's interf
 that path: grids, interpolation inputs/catalogs, the CUDA backend's interpolation entry
 points and the neighbour-search queries.
 """
+__version__ = "0.2.0"
+
 from ._lib import ArgumentError, CapacityError, DeviceError, DimensionMismatch
 from .grids import (Cartesian, Cylindrical, GridBundle, LineSamples, PointSamples, Polar, Spherical,
                     StructuredGrid, coordinate_grid, flatten, restore_struct)
@@ -19,5 +21,7 @@ from .neighbor import (LBVH_find_nearest, LBVH_find_nearest_h, LBVH_probe_neighb
 
 from . import phantom
 from .phantom import MassFromColumn, MassFromParams, ParticleDataFrame, add_rho, read_phantom
+from . import gridio
+from .gridio import GridDataset, read_GridDataset, write_GridBundle, write_GridDataset
 
 __all__ = [n for n in dir() if not n.startswith("_")]
