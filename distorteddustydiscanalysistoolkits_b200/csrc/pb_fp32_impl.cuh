@@ -60,9 +60,6 @@ __device__ __forceinline__ void shape(float q, float &f, float &df)
     }
 }
 
-// support radius in units of h (the shapes vanish, with their derivatives, for q >= this)
-__host__ __device__ constexpr float ksupport(int k) { return k == 1 ? 2.5f : (k == 2 ? 3.f : 2.f); }
-
 __device__ __forceinline__ float ldexp_norm3(int k)
 {
     const float pi = 3.14159265358979f;
