@@ -113,3 +113,24 @@ def test_reference_errors(tmp_path):
     pb.write_GridDataset(pb.GridDataset(gb, {"grid_type": "PointSamples"}), tmp_path / "nodtype.h5")
     with pytest.raises(pb.ArgumentError, match="params missing :dtype"):
         pb.read_GridDataset(tmp_path / "nodtype.h5")
+
+
+def test_two_dimensional_grids_and_value_types(tmp_path):
+    g = np.random.default_rng(3)
+    coor = (g.normal(size=50), g.normal(size=50))
+    pts = pb.GridBundle([pb.PointSamples(g.normal(size=50), coor)], ["Σρ"])   # a UTF-8 name
+    params = {"empty": "", "big": 2 ** 62, "neg": -7, "tiny": 5e-324, "off": False}
+    pb.write_GridDataset(pb.GridDataset(pts, dict(params, dtype="Float64", grid_type="PointSamples")),
+                         tmp_path / "p2.h5")
+    gd = pb.read_GridDataset(tmp_path / "p2.h5")
+    assert list(gd.data.names) == ["Σρ"] and len(gd.data.grids[0].coor) == 2
+    for k, v in params.items():
+        assert gd.params[k] == v and type(gd.params[k]) is type(v)
+    tree = gridio._open_tree(memoryview((tmp_path / "p2.h5").read_bytes()))
+    assert list(tree["data"]["coord"].keys()) == ["x", "y"]
+    axes = (np.linspace(0, 1, 4), np.linspace(0, 2, 6))
+    st = pb.GridBundle([pb.StructuredGrid(g.normal(size=(4, 6)), axes)], ["s"])
+    pb.write_GridBundle(st, tmp_path / "s2.h5", code_units=UNITS)
+    back = pb.read_GridDataset(tmp_path / "s2.h5")
+    assert back.data.grids[0].size == (4, 6) and np.array_equal(back.data.grids[0].grid, st.grids[0].grid)
+    assert back.params["file_identifier"].startswith("FT:Partia:%s (CommonOutput): " % pb.__version__)
